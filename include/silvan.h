@@ -1,0 +1,240 @@
+/*
+ * silvan.h -- C-ABI of the B200 progressive-sampling betweenness estimator.
+ *
+ * The reference (SILVAN) has no in-process API: its boundary is the binary's
+ * command line (silvan/main.cpp:38-154) driving Probabilistic::run
+ * (silvan/src/Probabilistic.cpp:775-1139), which calls Sp_sampler::random_path
+ * once per sample (silvan/src/Sp_sampler.cpp:41-238).  The entry points below
+ * replace that chain one-for-one; each comment names the reference interface
+ * it stands in for.  Plain pointers and sizes only; the caller owns every
+ * host buffer, a handle owns its device memory.
+ *
+ * Conventions
+ *   - Every call returns int: SILVAN_OK (0) or a negative SILVAN_E_* code;
+ *     silvan_last_error() returns a message for the calling thread.
+ *   - Nothing traps.  Conditions under which the reference divides by zero
+ *     or loops for hours are reported as status codes.
+ *   - A job is bound to one CUDA stream.  Calls on one job are not
+ *     thread-safe; different jobs may be driven from different host threads.
+ */
+#ifndef SILVAN_H
+#define SILVAN_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes -------------------------------------------------------- */
+#define SILVAN_OK 0
+#define SILVAN_E_BADARG -1    /* invalid argument or handle                  */
+#define SILVAN_E_IO -2        /* graph file cannot be read                   */
+#define SILVAN_E_PARSE -3     /* node id the reference cannot represent      */
+#define SILVAN_E_OOM -4       /* device or host allocation failed            */
+#define SILVAN_E_CUDA -5      /* CUDA runtime error                          */
+#define SILVAN_E_OVERFLOW -6  /* wrapped 64-bit path count reached 0; the
+                                 reference divides by zero there
+                                 (silvan/src/Rand_gen.cpp:24)                */
+#define SILVAN_E_NP_CAP -7    /* alpha * W paths for one sample exceed the
+                                 job's cap (silvan/src/Sp_sampler.cpp:166-170
+                                 can ask for ~2^31 backtracks per sample)    */
+#define SILVAN_E_TIMEOUT -8   /* a bounded device wait expired               */
+#define SILVAN_E_CAPACITY -9  /* a per-round buffer is too small             */
+#define SILVAN_E_STATE -10    /* call out of order                           */
+#define SILVAN_E_NOGPU -11    /* no usable CUDA device                       */
+
+/* ---- handles ------------------------------------------------------------- */
+typedef struct silvan_graph_s *silvan_graph_t;
+typedef struct silvan_job_s *silvan_job_t;
+
+typedef struct {
+    uint32_t n;             /* nodes (1 + largest id)                       */
+    uint32_t n_components;  /* strongly connected components                */
+    uint64_t m;             /* directed edge entries (edges_num)            */
+    uint32_t diameter;      /* AllCCUpperBound diameter bound               */
+    int32_t directed;
+} silvan_graph_info_t;
+
+/* Execution forms of the sampling loop. */
+#define SILVAN_FORM_PLAIN 0    /* one launch sequence per 11-sample block   */
+#define SILVAN_FORM_BATCHED 1  /* persistent sampler per schedule interval  */
+
+/* Estimator parameters: the binary's flags (silvan/main.cpp:20-33,63-137). */
+typedef struct {
+    double eps;          /* accuracy, absolute (k == 0) or relative (k > 0) */
+    double delta;        /* confidence                                      */
+    uint32_t k;          /* -k: top-k relative mode when > 0                */
+    int32_t m_hat;       /* 0 disables m_hat (-m)                           */
+    double alpha;        /* -s: multi-path sampling rate (default 2.3)      */
+    int32_t alpha_given; /* -s or -a given: keeps alpha fixed in pass 2     */
+    int32_t form;        /* SILVAN_FORM_*                                   */
+    double a;            /* -a: empirical peeling base (default 2); <= 1 off */
+    uint64_t seed;       /* Philox key of the job (default 42)              */
+    double verbose;      /* -v: seconds between progress lines (default 60) */
+    uint32_t np_cap;     /* max paths per sample (0 = default 2^24)         */
+    uint32_t slots;      /* concurrent sampler slots (0 = autotuned)        */
+    uint32_t threads;    /* divisor of union_sample (0 = 1, parity mode)    */
+    uint32_t reserved;
+} silvan_params_t;
+
+/* Fills p with the reference defaults. */
+void silvan_params_default(silvan_params_t *p);
+
+/* Result of a finished run: the values the reference prints. */
+typedef struct {
+    uint64_t first_pass_samples; /* "First pass finished after N iteration" */
+    uint64_t num_samples;        /* pass-2 samples ("Finished after")       */
+    uint64_t vis_edges;          /* edges visited, both passes              */
+    uint64_t void_samples;       /* pass-2 void samples                     */
+    uint64_t backtracked_paths;  /* sum of num_paths over counted samples   */
+    uint32_t tau;
+    uint32_t diameter;
+    int32_t iteration_index;
+    int32_t num_partitions;
+    int32_t stop_reason;         /* 1 = eps condition, 2 = omega reached    */
+    uint32_t union_sample;
+    uint32_t numresults_topk;
+    uint32_t checks;             /* stopping-rule evaluations               */
+    double omega;
+    double first_stopping_samples;
+    double last_stopping_samples;
+    double alpha_sp_sampling;    /* alpha used in pass 2                    */
+    double eps_stop;             /* sup eps at the stop, -1 if none          */
+    double eps_final_topk;
+    double sup_bcest;            /* max approx / num_samples                */
+    double sup_emp_wimpy_var;    /* max wimpy / num_samples                 */
+    double max_num_samples;      /* m_hat after pass 1                      */
+    double time_total_s;         /* "Total time" window                     */
+    double time_first_pass_s;
+    double time_sampling_s;      /* device time in the sampler              */
+    double time_apply_s;         /* device time in counter application     */
+    double time_device_s;        /* device time of the whole run (events)   */
+    uint64_t ball_nodes;         /* nodes visited by all samples            */
+    uint64_t pred_entries;       /* predecessor entries of all samples      */
+    uint64_t kernel_launches;    /* kernels launched by the run             */
+} silvan_result_t;
+
+/* ---- graphs (reference: Graph, silvan/src/Graph.cpp) ------------------- */
+
+/* Graph(filename, directed) (silvan/src/Graph.cpp:37-90) followed by
+ * compute_cc + estimate_diameter (silvan/src/Graph.cpp:109-316), then the
+ * CSR and component ids are copied to the device. */
+int silvan_graph_load(const char *path, int directed, silvan_graph_t *out);
+
+/* Same, from host CSR arrays (rows ascending, unique).  in_off/in_adj are
+ * ignored for undirected graphs.  cc may be NULL, in which case the
+ * components and the diameter bound are computed on the host. */
+int silvan_graph_upload(uint32_t n, int directed, const uint64_t *out_off,
+                        const uint32_t *out_adj, const uint64_t *in_off,
+                        const uint32_t *in_adj, const uint32_t *cc,
+                        uint32_t n_components, uint32_t diameter,
+                        silvan_graph_t *out);
+
+int silvan_graph_info(silvan_graph_t g, silvan_graph_info_t *info);
+
+/* Host CSR of a loaded graph (out rows, then in rows; in rows alias the
+ * out rows for undirected graphs).  Sizes from silvan_graph_info. */
+int silvan_graph_csr(silvan_graph_t g, uint64_t *out_off, uint32_t *out_adj,
+                     uint64_t *in_off, uint32_t *in_adj, uint32_t *cc);
+
+int silvan_graph_destroy(silvan_graph_t g);
+
+/* ---- host-only ingest ------------------------------------------------------
+ * The same ingest without a device: edge-list parse, CSR, components and
+ * diameter bound (silvan/src/Graph.cpp:37-316).  Useful to prepare graphs on
+ * machines without a GPU; silvan_graph_from_host uploads one. */
+typedef struct silvan_host_graph_s *silvan_host_graph_t;
+int silvan_host_graph_load(const char *path, int directed, silvan_host_graph_t *out);
+int silvan_host_graph_from_pairs(const uint32_t *pairs, uint64_t count, int directed,
+                                 silvan_host_graph_t *out);
+int silvan_host_graph_info(silvan_host_graph_t g, silvan_graph_info_t *info);
+int silvan_host_graph_csr(silvan_host_graph_t g, uint64_t *out_off, uint32_t *out_adj,
+                          uint64_t *in_off, uint32_t *in_adj, uint32_t *cc);
+int silvan_host_graph_destroy(silvan_host_graph_t g);
+int silvan_graph_from_host(silvan_host_graph_t h, silvan_graph_t *out);
+
+/* ---- jobs (reference: Probabilistic, silvan/include/Probabilistic.h) ---- */
+
+/* Probabilistic(...) constructor: allocates the device counters. */
+int silvan_job_create(silvan_graph_t g, const silvan_params_t *p, silvan_job_t *out);
+
+/* Probabilistic::run(k, delta, err): pass 1, empirical peeling, bounds,
+ * pass 2 with the progressive stopping rule.  Status lines of the
+ * reference are written to `log` when it is not NULL. */
+int silvan_job_run(silvan_job_t j, silvan_result_t *res, void *log /* FILE* */);
+
+/* get_centrality(v) for every node: approx[v] / num_samples. */
+int silvan_read_estimates(silvan_job_t j, double *out, uint32_t n);
+
+/* Ranked output of top-k mode: the numresults_topk (node, estimate) pairs in
+ * ranking order (silvan/src/Probabilistic.cpp:1121-1127). */
+int silvan_read_topk(silvan_job_t j, uint32_t *nodes, double *values, uint32_t cap,
+                     uint32_t *count);
+
+/* Raw pass-2 counters: approx (double), emp_wimpy_vars (double), mcrade
+ * (int64, n x 25, node-major) and partition_index (int32).  Any pointer may
+ * be NULL. */
+int silvan_read_counters(silvan_job_t j, double *approx, double *wimpy, int64_t *mcrade,
+                         int32_t *partition_index);
+
+int silvan_job_destroy(silvan_job_t j);
+
+/* ---- step-wise interface ------------------------------------------------- */
+
+/* Progress of the sampling loop. */
+typedef struct {
+    uint64_t samples;       /* samples committed in the current pass        */
+    uint64_t void_samples;
+    uint64_t vis_edges;
+    uint64_t backtracked_paths;
+    int32_t pass;           /* 1 or 2                                       */
+    int32_t error;          /* first device status (SILVAN_E_*) or 0       */
+} silvan_status_t;
+
+/* Draws and commits samples of the current pass until `target` samples
+ * have been committed (one Probabilistic::one_round per sample,
+ * silvan/src/Probabilistic.cpp:468-559). */
+int silvan_run_rounds(silvan_job_t j, uint64_t target, silvan_status_t *st);
+
+/* ---- per-sample replay (parity hook) -------------------------------------- */
+
+/* Runs the device sampler for global sample indices [first, first+count)
+ * and returns, per sample, what Sp_sampler::random_path returns
+ * (silvan/src/Sp_sampler.cpp:41-238): path_length, num_paths, vis_edges and
+ * the path map (node -> count, ascending node id), concatenated in
+ * ent_node/ent_cnt with nent[i] entries for sample i.  sample_status[i] is 0
+ * or a SILVAN_E_* code for that sample.  Returns SILVAN_E_CAPACITY when
+ * ent_cap is too small (*ent_total then holds the size needed). */
+int silvan_replay_samples(silvan_graph_t g, uint64_t seed, uint32_t first, uint32_t count,
+                          double alpha, uint32_t np_cap, int32_t *path_length,
+                          int32_t *num_paths, uint64_t *vis_edges, uint32_t *nent,
+                          int32_t *sample_status, uint32_t *ent_node, int32_t *ent_cnt,
+                          uint64_t ent_cap, uint64_t *ent_total);
+
+/* ---- synthetic workloads --------------------------------------------------- */
+
+/* Generators of the measured workloads; they write at most cap (u, v) pairs
+ * to pairs[2*i], pairs[2*i+1] and return the count in *count (when the
+ * buffer is too small, *count is the size needed and SILVAN_E_CAPACITY is
+ * returned).  kind: 0 = BA(n=a, m=b), 1 = ER(n=a, mean degree=x),
+ * 2 = R-MAT(scale=a, edge factor=b, directed=c), 3 = grid(side=a, delete
+ * fraction x, shortcut fraction y). */
+int silvan_generate(int kind, uint32_t a, uint32_t b, uint32_t c, double x, double y,
+                    uint64_t seed, uint32_t *pairs, uint64_t cap, uint64_t *count);
+
+/* Builds a graph handle directly from (u, v) pairs with the loader's
+ * semantics (dedup, sorted rows, reverse edges when undirected). */
+int silvan_graph_from_pairs(const uint32_t *pairs, uint64_t count, int directed,
+                            silvan_graph_t *out);
+
+/* ---- misc ------------------------------------------------------------------ */
+const char *silvan_last_error(void);
+const char *silvan_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SILVAN_H */

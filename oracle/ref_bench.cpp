@@ -1,0 +1,131 @@
+// Test infrastructure (oracle / CPU baseline): times the reference's own
+// estimator -- silvan/src/*.cpp unmodified, including its MMIX LCG Rand_gen
+// and its OpenMP threads, compiled with the reference's flags -- on a graph
+// given as CSR.  Built into oracle/_ref/libsilvan_refbench.so by
+// oracle/Makefile; only bench.py's reference arm and CPU-baseline leg load it.
+//
+// The reference can only construct its graph from a file through std::set
+// insertion (silvan/src/Graph.cpp:37-90), which takes about a minute for a
+// 16M-edge R-MAT and lies outside its own "Total time" window
+// (silvan/src/Probabilistic.cpp:810).  The harness constructs the estimator
+// on a two-node file and then installs the CSR rows in the reference's own
+// per-node arrays, re-allocating the per-node counters for the real size.
+#include <cstdint>
+#include <cstdlib>
+#include <cstring>
+#include <cstdio>
+#include <iostream>
+#include <sstream>
+#include <string>
+#include <map>
+#include <set>
+#include <vector>
+#include <utility>
+#include <ctype.h>
+#include <unistd.h>
+#include <omp.h>
+
+#define private public
+#define protected public
+#include "Graph.h"
+#include "Sp_sampler.h"
+#include "Probabilistic.h"
+#undef private
+#undef protected
+
+namespace {
+struct CoutCapture {
+    std::ostringstream buf;
+    std::streambuf *old;
+    CoutCapture() { old = std::cout.rdbuf(buf.rdbuf()); }
+    ~CoutCapture() { std::cout.rdbuf(old); }
+};
+
+double last_value(const std::string &text, const std::string &pattern) {
+    size_t pos = text.rfind(pattern);
+    if (pos == std::string::npos) return -1.0;
+    return std::strtod(text.c_str() + pos + pattern.size(), nullptr);
+}
+
+uint32_t **rows(uint32_t n, const uint64_t *off, const uint32_t *adj, uint32_t **deg) {
+    uint32_t **r = (uint32_t **)malloc(sizeof(uint32_t *) * n);
+    *deg = (uint32_t *)malloc(sizeof(uint32_t) * n);
+    for (uint32_t i = 0; i < n; i++) {
+        uint32_t d = (uint32_t)(off[i + 1] - off[i]);
+        (*deg)[i] = d;
+        r[i] = (uint32_t *)malloc(sizeof(uint32_t) * (d ? d : 1));
+        std::memcpy(r[i], adj + off[i], sizeof(uint32_t) * d);
+    }
+    return r;
+}
+}  // namespace
+
+extern "C" int refbench_run(uint32_t n, int directed, const uint64_t *out_off,
+                            const uint32_t *out_adj, const uint64_t *in_off,
+                            const uint32_t *in_adj, double eps, double delta, uint32_t k,
+                            double alpha, int alpha_given, double a, int mhat, int threads,
+                            double *total_time, uint64_t *pass1, uint64_t *pass2,
+                            uint64_t *vis_edges, char *stdout_buf, uint64_t stdout_cap) {
+    if (threads > 0) omp_set_num_threads(threads);
+    char path[] = "/tmp/silvan_refbench_XXXXXX";
+    int fd = mkstemp(path);
+    if (fd < 0) return -1;
+    const char two[] = "0 1\n";
+    if (write(fd, two, sizeof(two) - 1) != (ssize_t)(sizeof(two) - 1)) {
+        close(fd);
+        return -1;
+    }
+    close(fd);
+    std::string text;
+    {
+        CoutCapture cap;
+        Probabilistic *p = new Probabilistic(std::string(path), directed != 0, 1.0, alpha,
+                                             alpha_given != 0, a, mhat != 0, std::string(""));
+        unlink(path);
+        // install the CSR in the reference's per-node arrays
+        for (uint32_t i = 0; i < p->nodes_num; i++) free(p->adj[i]);
+        free(p->adj);
+        free(p->degrees);
+        if (directed) {
+            for (uint32_t i = 0; i < p->nodes_num; i++) free(p->inc[i]);
+            free(p->inc);
+            free(p->in_degrees);
+        }
+        free(p->cc);
+        p->nodes_num = n;
+        p->edges_num = out_off[n];
+        p->adj = rows(n, out_off, out_adj, &p->degrees);
+        if (directed) {
+            p->inc = rows(n, in_off, in_adj, &p->in_degrees);
+        } else {
+            p->inc = p->adj;
+            p->in_degrees = p->degrees;
+        }
+        p->cc = (uint32_t *)malloc(sizeof(uint32_t) * n);
+        free(p->approx);
+        free(p->approx_toadd);
+        free(p->emp_wimpy_vars);
+        free(p->mcrade);
+        free(p->partition_index);
+        p->approx = (double *)calloc(n, sizeof(double));
+        p->approx_toadd = (double *)calloc(n, sizeof(double));
+        p->emp_wimpy_vars = (double *)calloc(n, sizeof(double));
+        p->mcrade = (int64_t *)calloc((uint64_t)n * p->mctrials, sizeof(int64_t));
+        p->partition_index = (int *)calloc(n, sizeof(int));
+        p->run(k, delta, eps);
+        *pass2 = p->num_samples;
+        *vis_edges = p->vis_edges;
+        text = cap.buf.str();
+        delete p;
+    }
+    *total_time = last_value(text, "Total time: ");
+    *pass1 = (uint64_t)last_value(text, "First pass finished after ");
+    if (stdout_buf && stdout_cap) {
+        size_t l = std::min<size_t>(stdout_cap - 1, text.size());
+        std::memcpy(stdout_buf, text.data(), l);
+        stdout_buf[l] = 0;
+    }
+    return 0;
+}
+
+extern "C" int refbench_max_threads() { return omp_get_max_threads(); }

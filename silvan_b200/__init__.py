@@ -1,0 +1,416 @@
+"""silvan_b200 -- B200-native progressive-sampling betweenness estimation.
+
+Python host side of the library: ctypes bindings of ``include/silvan.h``
+mirroring the reference's interface (``Probabilistic(graph, flags).run(k,
+delta, err)`` of silvan/include/Probabilistic.h:27-56 and the command line of
+silvan/main.cpp).  Every estimate is computed by the CUDA kernels in
+``libsilvan_b200.so``; there is no CPU path, and loading fails loudly when the
+library is missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "libsilvan_b200.so")
+CLI_PATH = os.path.join(PKG, "bin", "silvan")
+
+OK = 0
+E_BADARG, E_IO, E_PARSE, E_OOM, E_CUDA = -1, -2, -3, -4, -5
+E_OVERFLOW, E_NP_CAP, E_TIMEOUT, E_CAPACITY, E_STATE, E_NOGPU = -6, -7, -8, -9, -10, -11
+FORM_PLAIN, FORM_BATCHED = 0, 1
+TRIALS = 25
+
+# Every function declared in include/silvan.h.
+EXPORTS = [
+    "silvan_params_default", "silvan_graph_load", "silvan_graph_upload", "silvan_graph_info",
+    "silvan_graph_csr", "silvan_graph_destroy", "silvan_host_graph_load",
+    "silvan_host_graph_from_pairs", "silvan_host_graph_info", "silvan_host_graph_csr",
+    "silvan_host_graph_destroy", "silvan_graph_from_host", "silvan_job_create",
+    "silvan_job_run", "silvan_read_estimates", "silvan_read_topk", "silvan_read_counters",
+    "silvan_job_destroy", "silvan_run_rounds", "silvan_replay_samples", "silvan_generate",
+    "silvan_graph_from_pairs", "silvan_last_error", "silvan_version",
+]
+
+
+class SilvanError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{msg} (status {code})")
+        self.code = code
+
+
+class GraphInfo(C.Structure):
+    _fields_ = [("n", C.c_uint32), ("n_components", C.c_uint32), ("m", C.c_uint64),
+                ("diameter", C.c_uint32), ("directed", C.c_int32)]
+
+
+class Params(C.Structure):
+    _fields_ = [("eps", C.c_double), ("delta", C.c_double), ("k", C.c_uint32),
+                ("m_hat", C.c_int32), ("alpha", C.c_double), ("alpha_given", C.c_int32),
+                ("form", C.c_int32), ("a", C.c_double), ("seed", C.c_uint64),
+                ("verbose", C.c_double), ("np_cap", C.c_uint32), ("slots", C.c_uint32),
+                ("threads", C.c_uint32), ("reserved", C.c_uint32)]
+
+
+class Result(C.Structure):
+    _fields_ = [("first_pass_samples", C.c_uint64), ("num_samples", C.c_uint64),
+                ("vis_edges", C.c_uint64), ("void_samples", C.c_uint64),
+                ("backtracked_paths", C.c_uint64), ("tau", C.c_uint32),
+                ("diameter", C.c_uint32), ("iteration_index", C.c_int32),
+                ("num_partitions", C.c_int32), ("stop_reason", C.c_int32),
+                ("union_sample", C.c_uint32), ("numresults_topk", C.c_uint32),
+                ("checks", C.c_uint32), ("omega", C.c_double),
+                ("first_stopping_samples", C.c_double), ("last_stopping_samples", C.c_double),
+                ("alpha_sp_sampling", C.c_double), ("eps_stop", C.c_double),
+                ("eps_final_topk", C.c_double), ("sup_bcest", C.c_double),
+                ("sup_emp_wimpy_var", C.c_double), ("max_num_samples", C.c_double),
+                ("time_total_s", C.c_double), ("time_first_pass_s", C.c_double),
+                ("time_sampling_s", C.c_double), ("time_apply_s", C.c_double),
+                ("time_device_s", C.c_double), ("ball_nodes", C.c_uint64),
+                ("pred_entries", C.c_uint64), ("kernel_launches", C.c_uint64)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+class Status(C.Structure):
+    _fields_ = [("samples", C.c_uint64), ("void_samples", C.c_uint64), ("vis_edges", C.c_uint64),
+                ("backtracked_paths", C.c_uint64), ("pass_", C.c_int32), ("error", C.c_int32)]
+
+
+_lib = None
+
+
+def load(path: str = LIB_PATH):
+    """Loads the native library (building nothing; see silvan_b200.build)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError(f"{path} is missing: build it with `python -m silvan_b200.build`")
+    lib = C.CDLL(path)
+    P = C.c_void_p
+    sig = {
+        "silvan_params_default": (None, [P]),
+        "silvan_graph_load": (C.c_int, [C.c_char_p, C.c_int, P]),
+        "silvan_graph_upload": (C.c_int, [C.c_uint32, C.c_int, P, P, P, P, P, C.c_uint32,
+                                          C.c_uint32, P]),
+        "silvan_graph_info": (C.c_int, [P, P]),
+        "silvan_graph_csr": (C.c_int, [P, P, P, P, P, P]),
+        "silvan_graph_destroy": (C.c_int, [P]),
+        "silvan_host_graph_load": (C.c_int, [C.c_char_p, C.c_int, P]),
+        "silvan_host_graph_from_pairs": (C.c_int, [P, C.c_uint64, C.c_int, P]),
+        "silvan_host_graph_info": (C.c_int, [P, P]),
+        "silvan_host_graph_csr": (C.c_int, [P, P, P, P, P, P]),
+        "silvan_host_graph_destroy": (C.c_int, [P]),
+        "silvan_graph_from_host": (C.c_int, [P, P]),
+        "silvan_graph_from_pairs": (C.c_int, [P, C.c_uint64, C.c_int, P]),
+        "silvan_job_create": (C.c_int, [P, P, P]),
+        "silvan_job_run": (C.c_int, [P, P, P]),
+        "silvan_run_rounds": (C.c_int, [P, C.c_uint64, P]),
+        "silvan_read_estimates": (C.c_int, [P, P, C.c_uint32]),
+        "silvan_read_topk": (C.c_int, [P, P, P, C.c_uint32, P]),
+        "silvan_read_counters": (C.c_int, [P, P, P, P, P]),
+        "silvan_job_destroy": (C.c_int, [P]),
+        "silvan_replay_samples": (C.c_int, [P, C.c_uint64, C.c_uint32, C.c_uint32, C.c_double,
+                                            C.c_uint32, P, P, P, P, P, P, P, C.c_uint64, P]),
+        "silvan_generate": (C.c_int, [C.c_int, C.c_uint32, C.c_uint32, C.c_uint32, C.c_double,
+                                      C.c_double, C.c_uint64, P, C.c_uint64, P]),
+        "silvan_last_error": (C.c_char_p, []),
+        "silvan_version": (C.c_char_p, []),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _p(a):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def _check(rc):
+    if rc != OK:
+        raise SilvanError(rc, load().silvan_last_error().decode())
+
+
+# ---- synthetic workloads ----------------------------------------------------------
+
+GEN_BA, GEN_ER, GEN_RMAT, GEN_GRID = 0, 1, 2, 3
+
+
+def generate(kind, a=0, b=0, c=0, x=0.0, y=0.0, seed=1):
+    """Edge pairs (uint32 array of shape (E, 2)) of a synthetic workload."""
+    lib = load()
+    cnt = C.c_uint64(0)
+    rc = lib.silvan_generate(kind, a, b, c, x, y, seed, None, 0, C.byref(cnt))
+    if rc not in (OK, E_CAPACITY):
+        _check(rc)
+    pairs = np.zeros((max(cnt.value, 1), 2), np.uint32)
+    _check(lib.silvan_generate(kind, a, b, c, x, y, seed, _p(pairs), cnt.value, C.byref(cnt)))
+    return pairs[:cnt.value]
+
+
+def barabasi_albert(n, m, seed):
+    return generate(GEN_BA, n, m, seed=seed)
+
+
+def erdos_renyi(n, mean_degree, seed):
+    return generate(GEN_ER, n, x=mean_degree, seed=seed)
+
+
+def rmat(scale, edge_factor, seed, directed):
+    return generate(GEN_RMAT, scale, edge_factor, int(directed), seed=seed)
+
+
+def grid(side, delete_frac, shortcut_frac, seed):
+    return generate(GEN_GRID, side, x=delete_frac, y=shortcut_frac, seed=seed)
+
+
+def write_edge_list(path, pairs):
+    with open(path, "w") as f:
+        f.write("".join(f"{u} {v}\n" for u, v in pairs.tolist()))
+
+
+# ---- graphs -------------------------------------------------------------------------
+
+
+@dataclass
+class CSR:
+    n: int
+    directed: bool
+    out_off: np.ndarray
+    out_adj: np.ndarray
+    in_off: np.ndarray
+    in_adj: np.ndarray
+    cc: np.ndarray
+    n_components: int
+    diameter: int
+
+
+class HostGraph:
+    """Host-only ingest (Graph(filename, directed) + compute_cc +
+    estimate_diameter of silvan/src/Graph.cpp) -- no device needed."""
+
+    def __init__(self, handle):
+        self.h = handle
+
+    @classmethod
+    def load(cls, path, directed=False):
+        h = C.c_void_p()
+        _check(load().silvan_host_graph_load(str(path).encode(), int(directed), C.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def from_pairs(cls, pairs, directed=False):
+        pairs = np.ascontiguousarray(pairs, np.uint32).reshape(-1, 2)
+        h = C.c_void_p()
+        _check(load().silvan_host_graph_from_pairs(_p(pairs), len(pairs), int(directed),
+                                                   C.byref(h)))
+        return cls(h)
+
+    def info(self):
+        i = GraphInfo()
+        _check(load().silvan_host_graph_info(self.h, C.byref(i)))
+        return i
+
+    def csr(self) -> CSR:
+        i = self.info()
+        n = i.n
+        oo = np.zeros(n + 1, np.uint64)
+        io = np.zeros(n + 1, np.uint64)
+        load().silvan_host_graph_csr(self.h, _p(oo), None, _p(io), None, None)
+        oa = np.zeros(max(int(oo[-1]), 1), np.uint32)
+        ia = np.zeros(max(int(io[-1]), 1), np.uint32)
+        cc = np.zeros(n, np.uint32)
+        _check(load().silvan_host_graph_csr(self.h, _p(oo), _p(oa), _p(io), _p(ia), _p(cc)))
+        return CSR(n, bool(i.directed), oo, oa[:int(oo[-1])], io, ia[:int(io[-1])], cc,
+                   i.n_components, i.diameter)
+
+    def __del__(self):
+        try:
+            if self.h:
+                load().silvan_host_graph_destroy(self.h)
+        except Exception:
+            pass
+
+
+class Graph:
+    """A graph resident on the device (CSR + component ids)."""
+
+    def __init__(self, handle):
+        self.h = handle
+        self._info = self.info()
+
+    @classmethod
+    def load(cls, path, directed=False):
+        h = C.c_void_p()
+        _check(load().silvan_graph_load(str(path).encode(), int(directed), C.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def from_pairs(cls, pairs, directed=False):
+        pairs = np.ascontiguousarray(pairs, np.uint32).reshape(-1, 2)
+        h = C.c_void_p()
+        _check(load().silvan_graph_from_pairs(_p(pairs), len(pairs), int(directed), C.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def from_host(cls, hg: HostGraph):
+        h = C.c_void_p()
+        _check(load().silvan_graph_from_host(hg.h, C.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def upload(cls, csr: CSR, with_cc=True):
+        h = C.c_void_p()
+        _check(load().silvan_graph_upload(
+            csr.n, int(csr.directed), _p(csr.out_off), _p(csr.out_adj),
+            _p(csr.in_off) if csr.directed else None, _p(csr.in_adj) if csr.directed else None,
+            _p(csr.cc) if with_cc else None, csr.n_components, csr.diameter, C.byref(h)))
+        return cls(h)
+
+    def info(self):
+        i = GraphInfo()
+        _check(load().silvan_graph_info(self.h, C.byref(i)))
+        return i
+
+    @property
+    def n(self):
+        return self._info.n
+
+    @property
+    def diameter(self):
+        return self._info.diameter
+
+    def csr(self) -> CSR:
+        i = self._info
+        n = i.n
+        oo = np.zeros(n + 1, np.uint64)
+        io = np.zeros(n + 1, np.uint64)
+        load().silvan_graph_csr(self.h, _p(oo), None, _p(io), None, None)
+        oa = np.zeros(max(int(oo[-1]), 1), np.uint32)
+        ia = np.zeros(max(int(io[-1]), 1), np.uint32)
+        cc = np.zeros(n, np.uint32)
+        _check(load().silvan_graph_csr(self.h, _p(oo), _p(oa), _p(io), _p(ia), _p(cc)))
+        return CSR(n, bool(i.directed), oo, oa[:int(oo[-1])], io, ia[:int(io[-1])], cc,
+                   i.n_components, i.diameter)
+
+    def replay(self, seed, first, count, alpha, np_cap=0):
+        """Per-sample output of the device sampler for samples
+        [first, first+count) (Sp_sampler::random_path, silvan/src/Sp_sampler.cpp:41)."""
+        lib = load()
+        pl = np.zeros(count, np.int32)
+        npth = np.zeros(count, np.int32)
+        vis = np.zeros(count, np.uint64)
+        nent = np.zeros(count, np.uint32)
+        st = np.zeros(count, np.int32)
+        tot = C.c_uint64(0)
+        cap = max(1 << 16, count * 32)
+        while True:
+            node = np.zeros(cap, np.uint32)
+            cnt = np.zeros(cap, np.int32)
+            rc = lib.silvan_replay_samples(self.h, seed, first, count, alpha, np_cap, _p(pl),
+                                           _p(npth), _p(vis), _p(nent), _p(st), _p(node),
+                                           _p(cnt), cap, C.byref(tot))
+            if rc == E_CAPACITY and tot.value > cap:
+                cap = int(tot.value)
+                continue
+            _check(rc)
+            break
+        e = int(tot.value)
+        off = np.zeros(count + 1, np.int64)
+        off[1:] = np.cumsum(nent.astype(np.int64))
+        return dict(path_length=pl, num_paths=npth, vis_edges=vis, offsets=off,
+                    nodes=node[:e].copy(), counts=cnt[:e].copy(), status=st)
+
+    def __del__(self):
+        try:
+            if self.h:
+                load().silvan_graph_destroy(self.h)
+        except Exception:
+            pass
+
+
+class Probabilistic:
+    """Mirror of the reference's estimator object (silvan/include/
+    Probabilistic.h:27-56): construct with the graph and the binary's flags,
+    call run(), read the centralities."""
+
+    def __init__(self, graph: Graph, eps, delta, k=0, alpha=2.3, alpha_given=False, a=2.0,
+                 m_hat=True, seed=42, form="batched", verbose=0.0, np_cap=0, slots=0,
+                 threads=1):
+        lib = load()
+        p = Params()
+        lib.silvan_params_default(C.byref(p))
+        p.eps, p.delta, p.k = eps, delta, k
+        p.alpha, p.alpha_given, p.a = alpha, int(alpha_given), a
+        p.m_hat, p.seed, p.verbose = int(m_hat), seed, verbose
+        p.form = FORM_PLAIN if form == "plain" else FORM_BATCHED
+        p.np_cap, p.slots, p.threads = np_cap, slots, threads
+        self.graph = graph
+        self.params = p
+        h = C.c_void_p()
+        _check(lib.silvan_job_create(graph.h, C.byref(p), C.byref(h)))
+        self.h = h
+        self.result = None
+
+    def run(self, log=None):
+        """Probabilistic::run: returns the result fields as a dict.  `log` may
+        be an open file to receive the reference's status lines."""
+        lib = load()
+        res = Result()
+        fp = None
+        if log is not None:
+            libc = C.CDLL(None)
+            libc.fdopen.restype = C.c_void_p
+            libc.fdopen.argtypes = [C.c_int, C.c_char_p]
+            log.flush()
+            fp = libc.fdopen(os.dup(log.fileno()), b"w")
+        try:
+            _check(lib.silvan_job_run(self.h, C.byref(res), fp))
+        finally:
+            if fp:
+                libc.fflush(C.c_void_p(fp))
+                libc.fclose.argtypes = [C.c_void_p]
+                libc.fclose(fp)
+        self.result = res.as_dict()
+        return self.result
+
+    def get_centrality(self):
+        """approx[v] / num_samples for every node."""
+        n = self.graph.n
+        out = np.zeros(n, np.float64)
+        _check(load().silvan_read_estimates(self.h, _p(out), n))
+        return out
+
+    def counters(self):
+        n = self.graph.n
+        approx = np.zeros(n, np.float64)
+        wimpy = np.zeros(n, np.float64)
+        mcrade = np.zeros(n * TRIALS, np.int64)
+        part = np.zeros(n, np.int32)
+        _check(load().silvan_read_counters(self.h, _p(approx), _p(wimpy), _p(mcrade), _p(part)))
+        return dict(approx=approx, wimpy=wimpy, mcrade=mcrade.reshape(n, TRIALS),
+                    partition_index=part)
+
+    def topk(self):
+        cap = max(1, (self.result or {}).get("numresults_topk", 0) + 1)
+        nodes = np.zeros(cap, np.uint32)
+        vals = np.zeros(cap, np.float64)
+        cnt = C.c_uint32(0)
+        _check(load().silvan_read_topk(self.h, _p(nodes), _p(vals), cap, C.byref(cnt)))
+        return nodes[:cnt.value], vals[:cnt.value]
+
+    def __del__(self):
+        try:
+            if getattr(self, "h", None):
+                load().silvan_job_destroy(self.h)
+        except Exception:
+            pass

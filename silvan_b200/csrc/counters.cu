@@ -1,0 +1,474 @@
+// Ordered commit of sample contributions (see counters.cuh).
+//
+// The reference adds every sample's path map to the per-node counters inside
+// one critical section, in sample order (silvan/src/Probabilistic.cpp:479-544):
+//   x = count * (1 / num_paths)
+//   approx[u] += x;  emp_wimpy_vars[u] += x * x;
+//   mcrade[u][j] = (int64)((double)mcrade[u][j] + sign_j * x)   (truncation)
+// With num_paths > 1 the additions are not associative, so a node's updates
+// must be applied in sample order.  A round's records are grouped by node
+// (count, scan, scatter), each node's group is sorted by sample index (a warp
+// bitonic sort for groups of <= 32, a CTA sort in shared memory otherwise)
+// and the group is folded sequentially: lanes 0..24 each carry one Monte
+// Carlo trial, lane 25 approx, lane 26 the wimpy variance.  Different nodes
+// are independent, so the only serial work is per node.
+#include <cfloat>
+
+#include "counters.cuh"
+
+namespace silvan {
+
+namespace {
+
+constexpr int kScanBlocks = 296;
+constexpr int kScanThreads = 256;
+
+__device__ __forceinline__ uint32_t round_records(const RoundBuffers &rb) {
+    unsigned long long c = *rb.rec_cursor;
+    return (uint32_t)(c < rb.rec_cap ? c : rb.rec_cap);
+}
+
+__global__ void signs_kernel(RoundBuffers rb, ApplyArgs a) {
+    for (uint32_t s = a.lo + blockIdx.x * blockDim.x + threadIdx.x; s < a.hi;
+         s += gridDim.x * blockDim.x)
+        rb.signs[s] = rademacher_mask(a.seed, a.first_sample + s);
+}
+
+__global__ void bucket_count_kernel(RoundBuffers rb, ApplyArgs a) {
+    const uint32_t R = round_records(rb);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < R; i += gridDim.x * blockDim.x) {
+        PathRec r = rb.recs[i];
+        if (r.sample < a.lo || r.sample >= a.hi) continue;
+        if (atomicAdd(&rb.node_cnt[r.node], 1u) == 0u) {
+            uint32_t t = atomicAdd(rb.n_touched, 1u);
+            rb.touched[t] = r.node;
+        }
+    }
+}
+
+// Three-step exclusive scan of node_cnt over the touched list; each block owns
+// a contiguous range of the list.
+__device__ __forceinline__ void range_of(uint32_t T, uint32_t &b, uint32_t &e) {
+    uint32_t per = (T + gridDim.x - 1) / gridDim.x;
+    b = min(T, blockIdx.x * per);
+    e = min(T, b + per);
+}
+
+__device__ uint32_t block_sum(uint32_t v, uint32_t *tmp) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) tmp[threadIdx.x >> 5] = v;
+    __syncthreads();
+    uint32_t t = 0;
+    if (threadIdx.x == 0) {
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += tmp[w];
+        tmp[0] = t;
+    }
+    __syncthreads();
+    t = tmp[0];
+    __syncthreads();
+    return t;
+}
+
+__global__ void scan_reduce_kernel(RoundBuffers rb) {
+    __shared__ uint32_t tmp[32];
+    const uint32_t T = *rb.n_touched;
+    uint32_t b, e;
+    range_of(T, b, e);
+    uint32_t s = 0;
+    for (uint32_t i = b + threadIdx.x; i < e; i += blockDim.x) s += rb.node_cnt[rb.touched[i]];
+    s = block_sum(s, tmp);
+    if (threadIdx.x == 0) rb.block_sums[blockIdx.x] = s;
+}
+
+__global__ void scan_top_kernel(RoundBuffers rb, int nblocks) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        uint32_t acc = 0;
+        for (int i = 0; i < nblocks; i++) {
+            uint32_t t = rb.block_sums[i];
+            rb.block_sums[i] = acc;
+            acc += t;
+        }
+        rb.block_sums[nblocks] = acc;
+    }
+}
+
+__global__ void scan_down_kernel(RoundBuffers rb) {
+    __shared__ uint32_t tmp[33];
+    const uint32_t T = *rb.n_touched;
+    uint32_t b, e;
+    range_of(T, b, e);
+    uint32_t carry = rb.block_sums[blockIdx.x];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (uint32_t c0 = b; c0 < e; c0 += blockDim.x) {
+        uint32_t i = c0 + threadIdx.x;
+        uint32_t node = 0, v = 0;
+        if (i < e) {
+            node = rb.touched[i];
+            v = rb.node_cnt[node];
+        }
+        uint32_t incl = v;
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += t;
+        }
+        if (lane == 31) tmp[warp] = incl;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            uint32_t acc = 0;
+            for (int w = 0; w < nw; w++) {
+                uint32_t t = tmp[w];
+                tmp[w] = acc;
+                acc += t;
+            }
+            tmp[32] = acc;
+        }
+        __syncthreads();
+        const uint32_t excl = carry + tmp[warp] + incl - v;
+        if (i < e) {
+            rb.bucket_off[i] = excl;
+            rb.node_cnt[node] = excl;  // becomes the scatter cursor
+        }
+        carry += tmp[32];
+        __syncthreads();
+    }
+    if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) rb.bucket_off[T] = rb.block_sums[gridDim.x];
+}
+
+__global__ void bucket_scatter_kernel(RoundBuffers rb, ApplyArgs a) {
+    const uint32_t R = round_records(rb);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < R; i += gridDim.x * blockDim.x) {
+        PathRec r = rb.recs[i];
+        if (r.sample < a.lo || r.sample >= a.hi) continue;
+        uint32_t pos = atomicAdd(&rb.node_cnt[r.node], 1u);
+        rb.entries[pos] = ((unsigned long long)r.sample << 32) | r.count;
+    }
+}
+
+__device__ __forceinline__ void atomic_max_nonneg_double(unsigned long long *p, double v) {
+    atomicMax(p, (unsigned long long)__double_as_longlong(v));
+}
+
+// Sequential fold of one node's sorted contributions.  Lane j < 25 carries
+// trial j of mcrade, lane 25 approx (and the top-k mark), lane 26 the wimpy
+// variance.  get(r) returns the r-th (sample << 32 | count) entry.
+template <typename Get>
+__device__ void fold_node(const RoundBuffers &rb, const JobCounters &jc, const ApplyArgs &a,
+                          uint32_t node, uint32_t b, Get get) {
+    const int lane = threadIdx.x & 31;
+    if (lane < kTrials) {
+        if (a.pass != 2) return;
+        long long *mp = &jc.mcrade[(uint64_t)node * kTrials + lane];
+        long long m = *mp;
+        for (uint32_t r = 0; r < b; r++) {
+            const unsigned long long e = get(r);
+            const uint32_t sl = (uint32_t)(e >> 32);
+            const uint32_t c = (uint32_t)e;
+            const double x = __dmul_rn((double)c, __ddiv_rn(1.0, (double)rb.np[sl]));
+            const bool plus = (rb.signs[sl] >> lane) & 1u;
+            m = (long long)__double2ll_rz(__dadd_rn(__ll2double_rn(m), plus ? x : -x));
+        }
+        *mp = m;
+    } else if (lane == 25) {
+        double ap = jc.approx[node];
+        uint32_t lu = 0;
+        for (uint32_t r = 0; r < b; r++) {
+            const unsigned long long e = get(r);
+            const uint32_t sl = (uint32_t)(e >> 32);
+            const uint32_t c = (uint32_t)e;
+            const double x = __dmul_rn((double)c, __ddiv_rn(1.0, (double)rb.np[sl]));
+            if (x > 0.) {
+                ap = __dadd_rn(ap, x);
+                lu = a.first_sample + sl + 1u;
+                if (a.track_cross && !jc.cross_flag[node] && ap >= 3.0) {
+                    jc.cross_flag[node] = 1;
+                    uint32_t k = atomicAdd(&jc.sc->n_cross, 1u);
+                    jc.cross_sample[k] = a.first_sample + sl;
+                }
+            }
+        }
+        jc.approx[node] = ap;
+        if (lu) jc.last_upd[node] = lu;
+        atomic_max_nonneg_double(&jc.sc->sup_approx_bits, ap);
+    } else if (lane == 26) {
+        double w = jc.wimpy[node];
+        for (uint32_t r = 0; r < b; r++) {
+            const unsigned long long e = get(r);
+            const uint32_t sl = (uint32_t)(e >> 32);
+            const uint32_t c = (uint32_t)e;
+            const double x = __dmul_rn((double)c, __ddiv_rn(1.0, (double)rb.np[sl]));
+            if (x > 0.) w = __dadd_rn(w, __dmul_rn(x, x));
+        }
+        jc.wimpy[node] = w;
+        atomic_max_nonneg_double(&jc.sc->sup_wimpy_bits, w);
+    }
+}
+
+__device__ __forceinline__ void warp_bitonic_sort(unsigned long long &key) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int k = 2; k <= 32; k <<= 1) {
+#pragma unroll
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            const unsigned long long o = __shfl_xor_sync(0xffffffffu, key, j);
+            const bool take_min = ((lane & j) == 0) == ((lane & k) == 0);
+            key = take_min ? (key < o ? key : o) : (key > o ? key : o);
+        }
+    }
+}
+
+constexpr int kApplyThreads = 256;
+
+// Groups of at most 32 entries: one warp per node.
+__global__ void __launch_bounds__(kApplyThreads) apply_small_kernel(RoundBuffers rb, JobCounters jc,
+                                                                     ApplyArgs a) {
+    __shared__ unsigned long long buf[kApplyThreads / 32][32];
+    const uint32_t T = *rb.n_touched;
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const uint32_t gw = blockIdx.x * (blockDim.x >> 5) + wib;
+    const uint32_t nw = gridDim.x * (blockDim.x >> 5);
+    for (uint32_t t = gw; t < T; t += nw) {
+        const uint32_t b0 = rb.bucket_off[t];
+        const uint32_t b = rb.bucket_off[t + 1] - b0;
+        if (b > 32) continue;
+        const uint32_t node = rb.touched[t];
+        unsigned long long key = (uint32_t)lane < b ? rb.entries[b0 + lane] : ~0ull;
+        warp_bitonic_sort(key);
+        buf[wib][lane] = key;
+        __syncwarp();
+        fold_node(rb, jc, a, node, b, [&](uint32_t r) { return buf[wib][r]; });
+        __syncwarp();
+    }
+}
+
+// Groups of more than 32 entries: one CTA per node, bitonic sort in shared
+// memory (groups are bounded by kLargeBucket through the sub-round size).
+__global__ void __launch_bounds__(1024) apply_large_kernel(RoundBuffers rb, JobCounters jc,
+                                                           ApplyArgs a) {
+    extern __shared__ unsigned long long sbuf[];
+    const uint32_t T = *rb.n_touched;
+    for (uint32_t t = blockIdx.x; t < T; t += gridDim.x) {
+        const uint32_t b0 = rb.bucket_off[t];
+        const uint32_t b = rb.bucket_off[t + 1] - b0;
+        if (b <= 32) continue;
+        if (b > kLargeBucket) {
+            if (threadIdx.x == 0) atomicCAS(&jc.sc->error, 0, SILVAN_E_CAPACITY);
+            continue;
+        }
+        uint32_t P = 64;
+        while (P < b) P <<= 1;
+        for (uint32_t i = threadIdx.x; i < P; i += blockDim.x)
+            sbuf[i] = i < b ? rb.entries[b0 + i] : ~0ull;
+        __syncthreads();
+        for (uint32_t k = 2; k <= P; k <<= 1) {
+            for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+                for (uint32_t i = threadIdx.x; i < P; i += blockDim.x) {
+                    const uint32_t l = i ^ j;
+                    if (l > i) {
+                        const unsigned long long x = sbuf[i], y = sbuf[l];
+                        const bool asc = (i & k) == 0;
+                        if (asc ? (x > y) : (x < y)) {
+                            sbuf[i] = y;
+                            sbuf[l] = x;
+                        }
+                    }
+                }
+                __syncthreads();
+            }
+        }
+        if (threadIdx.x < 32) {
+            const uint32_t node = rb.touched[t];
+            fold_node(rb, jc, a, node, b, [&](uint32_t r) { return sbuf[r]; });
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void commit_kernel(RoundBuffers rb, JobCounters jc, ApplyArgs a) {
+    unsigned long long vis = 0, cnt = 0, vd = 0, paths = 0, ball = 0, pred = 0;
+    for (uint32_t s = a.lo + blockIdx.x * blockDim.x + threadIdx.x; s < a.hi;
+         s += gridDim.x * blockDim.x) {
+        const int32_t st = rb.status[s];
+        if (st != 0) atomicCAS(&jc.sc->error, 0, st);
+        vis += rb.vis[s];
+        ball += rb.ball[s];
+        pred += rb.pred[s];
+        const int32_t pl = rb.pl[s];
+        if (pl > 0) {
+            if ((uint32_t)pl <= a.D) atomicAdd((unsigned long long *)&jc.sp_lengths[pl], 1ull);
+            else atomicCAS(&jc.sc->error, 0, SILVAN_E_STATE);
+            cnt++;
+            paths += (unsigned long long)rb.np[s];
+        } else {
+            vd++;
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        vis += __shfl_xor_sync(0xffffffffu, vis, o);
+        cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+        vd += __shfl_xor_sync(0xffffffffu, vd, o);
+        paths += __shfl_xor_sync(0xffffffffu, paths, o);
+        ball += __shfl_xor_sync(0xffffffffu, ball, o);
+        pred += __shfl_xor_sync(0xffffffffu, pred, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (vis) atomicAdd(&jc.sc->vis_edges, vis);
+        if (cnt) atomicAdd(&jc.sc->counted_samples, cnt);
+        if (vd) atomicAdd(&jc.sc->void_samples, vd);
+        if (paths) atomicAdd(&jc.sc->paths, paths);
+        if (ball) atomicAdd(&jc.sc->ball_nodes, ball);
+        if (pred) atomicAdd(&jc.sc->pred_entries, pred);
+    }
+}
+
+__global__ void reset_touched_kernel(RoundBuffers rb) {
+    const uint32_t T = *rb.n_touched;
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < T; t += gridDim.x * blockDim.x)
+        rb.node_cnt[rb.touched[t]] = 0;
+}
+
+__global__ void stop_init_kernel(StopReduction *out, int nparts, long long init) {
+    for (int i = threadIdx.x; i < nparts * kTrials; i += blockDim.x) out->mc_max[i] = init;
+    for (int i = threadIdx.x; i < nparts; i += blockDim.x) out->wimpy_max[i] = 0.0;
+    if (threadIdx.x == 0) {
+        out->approx_max = 0.0;
+        out->wimpy_all_max = 0.0;
+    }
+}
+
+__global__ void __launch_bounds__(512) stop_reduce_kernel(JobCounters jc, uint32_t n, int nparts,
+                                                          long long init, StopReduction *out) {
+    __shared__ long long smc[kMaxPartitions * kTrials];
+    __shared__ unsigned long long sw[kMaxPartitions];
+    for (int i = threadIdx.x; i < nparts * kTrials; i += blockDim.x) smc[i] = init;
+    for (int i = threadIdx.x; i < nparts; i += blockDim.x) sw[i] = 0ull;
+    __syncthreads();
+    const uint64_t total = (uint64_t)n * kTrials;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < total; i += stride) {
+        const uint32_t v = (uint32_t)(i / kTrials);
+        const uint32_t j = (uint32_t)(i - (uint64_t)v * kTrials);
+        const int p = jc.partition[v];
+        const long long m = jc.mcrade[i];
+        if (m > smc[p * kTrials + j]) atomicMax(&smc[p * kTrials + j], m);
+    }
+    unsigned long long amax = 0, wmax = 0;
+    for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < n; v += stride) {
+        const unsigned long long wb = (unsigned long long)__double_as_longlong(jc.wimpy[v]);
+        const unsigned long long ab = (unsigned long long)__double_as_longlong(jc.approx[v]);
+        const int p = jc.partition[v];
+        if (wb > sw[p]) atomicMax(&sw[p], wb);
+        amax = ab > amax ? ab : amax;
+        wmax = wb > wmax ? wb : wmax;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        unsigned long long x = __shfl_xor_sync(0xffffffffu, amax, o);
+        unsigned long long y = __shfl_xor_sync(0xffffffffu, wmax, o);
+        amax = x > amax ? x : amax;
+        wmax = y > wmax ? y : wmax;
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMax(reinterpret_cast<unsigned long long *>(&out->approx_max), amax);
+        atomicMax(reinterpret_cast<unsigned long long *>(&out->wimpy_all_max), wmax);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < nparts * kTrials; i += blockDim.x)
+        if (smc[i] != init) atomicMax(&out->mc_max[i], smc[i]);
+    for (int i = threadIdx.x; i < nparts; i += blockDim.x)
+        if (sw[i]) atomicMax(reinterpret_cast<unsigned long long *>(&out->wimpy_max[i]), sw[i]);
+}
+
+__global__ void peel_index_kernel(JobCounters jc, uint32_t n, double m, double a, uint32_t *unc,
+                                  uint32_t *n_unc, uint32_t cap) {
+    const double la = log(a);
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+        const double ew = jc.wimpy[v] / m;
+        const double mi = fmin(1. / ew, m);
+        const double t = log(mi) / la + 1;
+        jc.peel_idx[v] = (int)t;
+        // the C library's log may differ from the device's by an ulp; flag the
+        // nodes where that could move (int)t so the host recomputes them
+        const double fr = t - floor(t);
+        if (fr < 1e-9 || fr > 1.0 - 1e-9) {
+            uint32_t k = atomicAdd(n_unc, 1u);
+            if (k < cap) unc[k] = v;
+        }
+    }
+}
+
+__global__ void peel_hist_kernel(JobCounters jc, uint32_t n, int32_t idx_min, int32_t nbins,
+                                 uint32_t *hist) {
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+        int32_t b = jc.peel_idx[v] - idx_min;
+        b = b < 0 ? 0 : (b >= nbins ? nbins - 1 : b);
+        atomicAdd(&hist[b], 1u);
+    }
+}
+
+__global__ void peel_map_kernel(JobCounters jc, uint32_t n, const int32_t *lut, int32_t idx_min,
+                                int32_t lut_size) {
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+        int32_t b = jc.peel_idx[v] - idx_min;
+        b = b < 0 ? 0 : (b >= lut_size ? lut_size - 1 : b);
+        jc.partition[v] = lut[b];
+    }
+}
+
+}  // namespace
+
+cudaError_t apply_round(const RoundBuffers &rb, const JobCounters &jc, const ApplyArgs &a,
+                        cudaStream_t stream) {
+    static bool attr_done = false;
+    if (!attr_done) {
+        cudaFuncSetAttribute(apply_large_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)(kLargeBucket * sizeof(unsigned long long)));
+        attr_done = true;
+    }
+    cudaMemsetAsync(rb.n_touched, 0, sizeof(uint32_t), stream);
+    if (a.pass == 2) signs_kernel<<<64, 256, 0, stream>>>(rb, a);
+    bucket_count_kernel<<<592, 256, 0, stream>>>(rb, a);
+    scan_reduce_kernel<<<kScanBlocks, kScanThreads, 0, stream>>>(rb);
+    scan_top_kernel<<<1, 32, 0, stream>>>(rb, kScanBlocks);
+    scan_down_kernel<<<kScanBlocks, kScanThreads, 0, stream>>>(rb);
+    bucket_scatter_kernel<<<592, 256, 0, stream>>>(rb, a);
+    apply_small_kernel<<<592, kApplyThreads, 0, stream>>>(rb, jc, a);
+    apply_large_kernel<<<148, 1024, kLargeBucket * sizeof(unsigned long long), stream>>>(rb, jc, a);
+    commit_kernel<<<16, 256, 0, stream>>>(rb, jc, a);
+    reset_touched_kernel<<<148, 256, 0, stream>>>(rb);
+    return cudaGetLastError();
+}
+
+cudaError_t stop_reduce(const JobCounters &jc, uint32_t n, int nparts, long long init,
+                        StopReduction *out_dev, cudaStream_t stream) {
+    stop_init_kernel<<<1, 256, 0, stream>>>(out_dev, nparts, init);
+    stop_reduce_kernel<<<296, 512, 0, stream>>>(jc, n, nparts, init, out_dev);
+    return cudaGetLastError();
+}
+
+cudaError_t peel_index(const JobCounters &jc, uint32_t n, double num_samples, double a,
+                       uint32_t *uncertain, uint32_t *n_uncertain, uint32_t cap,
+                       cudaStream_t stream) {
+    cudaMemsetAsync(n_uncertain, 0, sizeof(uint32_t), stream);
+    peel_index_kernel<<<592, 256, 0, stream>>>(jc, n, num_samples, a, uncertain, n_uncertain, cap);
+    return cudaGetLastError();
+}
+
+cudaError_t peel_hist(const JobCounters &jc, uint32_t n, int32_t idx_min, int32_t nbins,
+                      uint32_t *hist, cudaStream_t stream) {
+    cudaMemsetAsync(hist, 0, sizeof(uint32_t) * nbins, stream);
+    peel_hist_kernel<<<592, 256, 0, stream>>>(jc, n, idx_min, nbins, hist);
+    return cudaGetLastError();
+}
+
+cudaError_t peel_map(const JobCounters &jc, uint32_t n, const int32_t *lut, int32_t idx_min,
+                     int32_t lut_size, uint32_t *hist, cudaStream_t stream) {
+    (void)hist;
+    peel_map_kernel<<<592, 256, 0, stream>>>(jc, n, lut, idx_min, lut_size);
+    return cudaGetLastError();
+}
+
+cudaError_t ranking_candidates(const JobCounters &, uint32_t, double, uint32_t *, uint32_t *,
+                               uint32_t, cudaStream_t) {
+    return cudaErrorNotSupported;
+}
+
+}  // namespace silvan

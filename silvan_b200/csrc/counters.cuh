@@ -1,0 +1,117 @@
+// Device counters of a job and the kernels that commit a round of samples to
+// them in the reference's sequential order (silvan/src/Probabilistic.cpp:
+// 468-559), reduce them for the stopping rule (:251-414) and partition the
+// nodes by empirical peeling (:853-871).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+
+namespace silvan {
+
+constexpr uint32_t kLargeBucket = 16384;  // samples per apply sub-round (bucket bound)
+constexpr int kMaxPartitions = 128;
+
+// Job-level scalars kept on the device.
+struct JobScalars {
+    unsigned long long sup_approx_bits;  // max approx (non-negative doubles as bits)
+    unsigned long long sup_wimpy_bits;   // max emp_wimpy_vars
+    unsigned long long vis_edges;
+    unsigned long long void_samples;
+    unsigned long long counted_samples;
+    unsigned long long paths;            // sum of num_paths over counted samples
+    unsigned long long ball_nodes;       // nodes visited by the samplers
+    unsigned long long pred_entries;     // predecessor entries recorded
+    int32_t error;                       // first SILVAN_E_* seen
+    uint32_t n_cross;                    // crossings of the top-k "approx >= 3" mark
+};
+
+struct RoundBuffers {
+    // per round-local sample
+    int32_t *pl;
+    int32_t *np;
+    uint64_t *vis;
+    int32_t *status;
+    uint32_t *signs;
+    uint32_t *ball;
+    uint32_t *pred;
+    uint32_t max_samples;
+    // path-map records
+    PathRec *recs;
+    unsigned long long *rec_cursor;
+    uint64_t rec_cap;
+    // bucketing by node
+    uint32_t *node_cnt;      // n, zero between rounds
+    uint32_t *touched;       // distinct nodes of the round
+    uint32_t *n_touched;
+    uint32_t *bucket_off;    // n_touched + 1
+    unsigned long long *entries;  // sample << 32 | count, grouped by node
+    uint32_t *block_sums;    // scan scratch
+    uint32_t *work_counter;  // sampler work counter
+};
+
+struct JobCounters {
+    double *approx;
+    double *wimpy;
+    long long *mcrade;    // n x 25, node-major
+    uint32_t *last_upd;   // 1 + global index of the last sample that updated the node
+    uint8_t *cross_flag;  // approx_toadd of the reference (top-k pass 1)
+    uint32_t *cross_sample;  // global sample index of each crossing
+    uint64_t *sp_lengths;    // D + 1
+    JobScalars *sc;
+    int32_t *partition;   // dense partition id per node
+    int32_t *peel_idx;    // raw peeling index per node
+};
+
+struct ApplyArgs {
+    uint32_t n;
+    uint64_t seed;
+    uint32_t first_sample;   // global index of round-local sample 0
+    uint32_t lo, hi;         // round-local sample range committed by this call
+    int pass;                // 1 or 2 (pass 2 updates mcrade)
+    int track_cross;         // pass 1 of top-k mode
+    uint32_t D;
+};
+
+// Kernels apply_round launches (one fewer in pass 1: no Rademacher signs).
+constexpr int kApplyRoundKernels = 10;
+
+// Commits round-local samples [lo, hi) of `rb` to `jc`.  Launches only; all
+// sizes that depend on the round are read on the device, so the sequence can
+// be captured in a CUDA graph.
+cudaError_t apply_round(const RoundBuffers &rb, const JobCounters &jc, const ApplyArgs &a,
+                        cudaStream_t stream);
+
+// Reduction for one stopping-rule evaluation: per partition and trial the
+// maximum of mcrade (initialised to -n_pairs), per partition the maximum of
+// emp_wimpy_vars, and the global maxima of approx and emp_wimpy_vars.
+struct StopReduction {
+    long long mc_max[kMaxPartitions * kTrials];
+    double wimpy_max[kMaxPartitions];
+    double approx_max;
+    double wimpy_all_max;
+};
+cudaError_t stop_reduce(const JobCounters &jc, uint32_t n, int nparts, long long init,
+                        StopReduction *out_dev, cudaStream_t stream);
+
+// Empirical peeling index of every node (Probabilistic.cpp:855-862), with the
+// nodes whose index is within rounding distance of a boundary listed so that
+// the host can recompute them with the C library's log.
+cudaError_t peel_index(const JobCounters &jc, uint32_t n, double num_samples, double a,
+                       uint32_t *uncertain, uint32_t *n_uncertain, uint32_t cap,
+                       cudaStream_t stream);
+cudaError_t peel_map(const JobCounters &jc, uint32_t n, const int32_t *lut, int32_t idx_min,
+                     int32_t lut_size, uint32_t *hist, cudaStream_t stream);
+cudaError_t peel_hist(const JobCounters &jc, uint32_t n, int32_t idx_min, int32_t nbins,
+                      uint32_t *hist, cudaStream_t stream);
+
+// Top-(k+1) value of approx (top-k mode, Probabilistic.cpp:949) is computed on
+// the host from the ranking; the ranking itself:
+//   order by (approx desc, last update desc, node desc), never-updated nodes
+//   after all updated ones in ascending id (the initial Ranking_list).
+cudaError_t ranking_candidates(const JobCounters &jc, uint32_t n, double threshold,
+                               uint32_t *out_nodes, uint32_t *out_count, uint32_t cap,
+                               cudaStream_t stream);
+
+}  // namespace silvan

@@ -1,0 +1,604 @@
+// Device s-t shortest-path sampler (see sampler.cuh).
+//
+// One CTA slot processes one sample at a time and takes the next round-local
+// sample index from a device counter, so a round of many samples runs as one
+// persistent launch (the batched form) and a round of 11 samples as a small
+// one (the plain form); both execute the same per-sample code.
+//
+// Exactness.  The reference expands a BFS level by scanning the frontier in
+// queue order and each adjacency row in ascending order
+// (silvan/src/Sp_sampler.cpp:116-140).  Its results depend on that order:
+// the first scan item that reaches a node fixes the node's queue position,
+// predecessor lists are appended in scan order, and meeting edges are
+// collected in scan order.  Here the items of a level are numbered
+// g = 0, 1, ... in exactly that order and processed in tiles of ascending g:
+//   phase 1  every item reads the state of its neighbour y; an unvisited y is
+//            claimed with a CAS, and every item that reaches a node of the new
+//            level records itself with atomicMin/atomicMax of (g << 32 | x)
+//            (the first and the last predecessor), a count and sigma += sigma(x)
+//            (a wrapping sum, order-free);
+//   phase 2  after a barrier the items whose g equals their node's minimum are
+//            the joining hits; they and the meeting items are compacted in g
+//            order (warp ballots plus one block scan), which appends new nodes
+//            to the queue and meeting edges to the list in the reference order.
+// A later tile can never lower a node's minimum below an earlier tile's g, so
+// each tile is final once its own phase 1 is done.
+//
+// The backtrack needs pred(y)[t] with t = min(r mod sigma(y), |pred(y)| - 1)
+// (Sp_sampler.cpp:241-265: the walk adds n_paths[v] == 1 per entry).  t == 0
+// is the first hit, t == |pred|-1 the last hit; any other t is resolved by
+// ranking the predecessors (reverse neighbours on the previous level of the
+// same side) by their own queue order.
+#include "sampler.cuh"
+
+namespace silvan {
+
+namespace {
+
+constexpr int kWarps = kSamplerBlock / 32;
+constexpr int kItems = 4;                      // scan items per lane per tile
+constexpr int kTile = kSamplerBlock * kItems;  // scan items per tile
+constexpr int kChunk = 2048;                   // frontier nodes staged at once
+
+struct SamplerSmem {
+    uint32_t f_node[kChunk];
+    uint32_t f_off[kChunk];
+    uint32_t f_pre[kChunk + 1];
+    unsigned long long f_sig[kChunk];
+    uint32_t warp_a[kWarps];
+    uint32_t warp_b[kWarps];
+    uint32_t scan_tmp[kWarps + 1];
+    unsigned long long wsum[kWarps];
+    unsigned long long rec_base;
+    uint32_t tile_n_base, tile_m_base, tile_n_tot, tile_m_tot;
+    uint32_t sum_new;
+    uint32_t pred_hits;
+    // sample state
+    uint32_t sample;  // round-local index, or >= count when done
+    uint32_t u, v, draw_base;
+    uint32_t end_q;
+    uint32_t start_u, end_u, start_v, end_v;
+    uint32_t sum_u, sum_v, depth_u, depth_v;
+    uint32_t nmeet, ntouched;
+    unsigned long long vis;
+    int32_t status;
+    int32_t nonmono;
+    unsigned long long W;
+    uint32_t chunk_total;
+};
+
+__device__ __forceinline__ uint32_t lanemask_lt() {
+    uint32_t m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+__device__ __forceinline__ uint32_t draw32(uint64_t seed, uint32_t sample, uint32_t d) {
+    return philox_lo32(seed, sample, kStreamSampler, d);
+}
+
+// Exclusive block scan of one value per thread; returns the block total.
+// tmp needs kWarps + 1 entries.
+__device__ uint32_t block_exclusive_scan(uint32_t v, uint32_t &excl, uint32_t *tmp) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t incl = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+    }
+    if (lane == 31) tmp[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        const uint32_t w = lane < kWarps ? tmp[lane] : 0u;
+        uint32_t wi = w;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t t = __shfl_up_sync(0xffffffffu, wi, o);
+            if (lane >= o) wi += t;
+        }
+        if (lane < kWarps) tmp[lane] = wi - w;
+        if (lane == kWarps - 1) tmp[kWarps] = wi;
+    }
+    __syncthreads();
+    excl = tmp[warp] + incl - v;
+    const uint32_t total = tmp[kWarps];
+    __syncthreads();
+    return total;
+}
+
+__device__ __forceinline__ void rec_reset(NodeRec *r) {
+    uint4 *p = reinterpret_cast<uint4 *>(r);
+    p[0] = make_uint4(0u, 0u, 0u, 0u);                  // st, cnt, sigma
+    p[1] = make_uint4(0xffffffffu, 0xffffffffu, 0u, 0u);  // first = ~0, last = 0
+}
+
+// Predecessor of rank t (queue order) of node a, 0 < t < cnt - 1.
+__device__ uint32_t middle_pred(const SamplerArgs &A, const NodeRec *rec, uint32_t a,
+                                uint32_t st_a, uint32_t t) {
+    const uint32_t side = st_side(st_a);
+    const uint32_t want = st_make(side, st_dist(st_a) - 1u);
+    const uint32_t *off = side == kSideU ? A.in_off : A.out_off;
+    const uint32_t *adj = side == kSideU ? A.in_adj : A.out_adj;
+    const uint32_t b = off[a], e = off[a + 1];
+    unsigned long long prev = 0;
+    bool have_prev = false;
+    uint32_t bx = a;
+    for (uint32_t r = 0; r <= t; r++) {
+        unsigned long long best = ~0ull;
+        for (uint32_t k = b; k < e; k++) {
+            uint32_t x = adj[k];
+            if (__ldcg(&rec[x].st) != want) continue;
+            unsigned long long key = __ldcg(&rec[x].first) >> 32;
+            if ((!have_prev || key > prev) && key < best) {
+                best = key;
+                bx = x;
+            }
+        }
+        prev = best;
+        have_prev = true;
+    }
+    return bx;
+}
+
+__device__ __forceinline__ void note_hit(uint32_t *hits, uint32_t *touched, SamplerSmem &s,
+                                         uint32_t a) {
+    if (atomicAdd(&hits[a], 1u) == 0u) {
+        uint32_t i = atomicAdd(&s.ntouched, 1u);
+        touched[i] = a;
+    }
+}
+
+// Expands one BFS level of `side` (silvan/src/Sp_sampler.cpp:89-143).
+__device__ void expand_level(const SamplerArgs &A, SamplerSmem &s, NodeRec *rec,
+                             uint32_t *queue, uint2 *meet, uint32_t side, uint32_t lo,
+                             uint32_t hi, uint32_t depth) {
+    const uint32_t *off = side == kSideU ? A.out_off : A.in_off;
+    const uint32_t *adj = side == kSideU ? A.out_adj : A.in_adj;
+    const uint32_t new_st = st_make(side, depth + 1u);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t gbase = 0;  // item number of the chunk's first item within the level
+    uint32_t sum_local = 0;
+    uint32_t hits_local = 0;
+    for (uint32_t c0 = lo; c0 < hi; c0 += kChunk) {
+        const uint32_t nc = min((uint32_t)kChunk, hi - c0);
+        // stage the chunk: row starts, degrees (prefix), sigma
+        uint32_t degs[kChunk / kSamplerBlock];
+        uint32_t tsum = 0;
+#pragma unroll
+        for (int i = 0; i < kChunk / kSamplerBlock; i++) {
+            uint32_t p = threadIdx.x * (kChunk / kSamplerBlock) + i;
+            uint32_t d = 0;
+            if (p < nc) {
+                uint32_t x = __ldcg(&queue[c0 + p]);
+                uint32_t o0 = off[x];
+                d = off[x + 1] - o0;
+                s.f_node[p] = x;
+                s.f_off[p] = o0;
+                s.f_sig[p] = __ldcg(&rec[x].sigma);
+            }
+            degs[i] = d;
+            tsum += d;
+        }
+        uint32_t excl;
+        uint32_t total = block_exclusive_scan(tsum, excl, s.scan_tmp);
+#pragma unroll
+        for (int i = 0; i < kChunk / kSamplerBlock; i++) {
+            uint32_t p = threadIdx.x * (kChunk / kSamplerBlock) + i;
+            if (p < nc) s.f_pre[p] = excl;
+            excl += degs[i];
+        }
+        if (threadIdx.x == 0) s.f_pre[nc] = total;
+        __syncthreads();
+        const uint32_t G = total;
+        for (uint32_t t0 = 0; t0 < G; t0 += kTile) {
+            // ---- phase 1 ------------------------------------------------------
+            uint32_t ys[kItems], xs[kItems], code[kItems];
+#pragma unroll
+            for (int k = 0; k < kItems; k++) {
+                uint32_t it = t0 + (uint32_t)(warp * 32 * kItems + k * 32 + lane);
+                code[k] = 0;
+                ys[k] = 0;
+                xs[k] = 0;
+                if (it < G) {
+                    uint32_t l = 0, h = nc;
+                    while (h - l > 1) {
+                        uint32_t mid = (l + h) >> 1;
+                        if (s.f_pre[mid] <= it) l = mid;
+                        else h = mid;
+                    }
+                    const uint32_t x = s.f_node[l];
+                    const uint32_t y = adj[s.f_off[l] + (it - s.f_pre[l])];
+                    xs[k] = x;
+                    ys[k] = y;
+                    uint32_t sty = __ldcg(&rec[y].st);
+                    if (sty == 0u) {
+                        atomicCAS(&rec[y].st, 0u, new_st);
+                        code[k] = 1;
+                    } else if (sty == new_st) {
+                        code[k] = 1;
+                    } else if (st_side(sty) != side) {
+                        code[k] = 2;
+                    }
+                    if (code[k] == 1) {
+                        const unsigned long long key =
+                            ((unsigned long long)(gbase + it) << 32) | x;
+                        atomicMin(reinterpret_cast<unsigned long long *>(&rec[y].first), key);
+                        atomicMax(reinterpret_cast<unsigned long long *>(&rec[y].last), key);
+                        atomicAdd(&rec[y].cnt, 1u);
+                        atomicAdd(reinterpret_cast<unsigned long long *>(&rec[y].sigma),
+                                  s.f_sig[l]);
+                    }
+                }
+            }
+            __syncthreads();
+            // ---- phase 2: ordered compaction of joins and meeting edges -------
+            uint32_t rn[kItems], rm[kItems];
+            uint32_t cn = 0, cm = 0;
+            uint32_t nhit = 0;
+#pragma unroll
+            for (int k = 0; k < kItems; k++) nhit += code[k] == 1 ? 1u : 0u;
+            hits_local += nhit;
+#pragma unroll
+            for (int k = 0; k < kItems; k++) {
+                uint32_t it = t0 + (uint32_t)(warp * 32 * kItems + k * 32 + lane);
+                bool win = false;
+                if (code[k] == 1) {
+                    unsigned long long f = __ldcg(
+                        reinterpret_cast<const unsigned long long *>(&rec[ys[k]].first));
+                    win = (uint32_t)(f >> 32) == gbase + it;
+                }
+                if (!win && code[k] == 1) code[k] = 0;
+                uint32_t bn = __ballot_sync(0xffffffffu, win);
+                uint32_t bm = __ballot_sync(0xffffffffu, code[k] == 2);
+                rn[k] = cn + __popc(bn & lanemask_lt());
+                rm[k] = cm + __popc(bm & lanemask_lt());
+                cn += __popc(bn);
+                cm += __popc(bm);
+            }
+            if (lane == 0) {
+                s.warp_a[warp] = cn;
+                s.warp_b[warp] = cm;
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                uint32_t an = 0, am = 0;
+                for (int w = 0; w < kWarps; w++) {
+                    uint32_t tn = s.warp_a[w], tm = s.warp_b[w];
+                    s.warp_a[w] = an;
+                    s.warp_b[w] = am;
+                    an += tn;
+                    am += tm;
+                }
+                s.tile_n_base = s.end_q;
+                s.tile_m_base = s.nmeet;
+                s.tile_n_tot = an;
+                s.tile_m_tot = am;
+                if (s.nmeet + am > kMeetCap && s.status == 0) s.status = SILVAN_E_CAPACITY;
+            }
+            __syncthreads();
+            const uint32_t nb = s.tile_n_base + s.warp_a[warp];
+            const uint32_t mb = s.tile_m_base + s.warp_b[warp];
+#pragma unroll
+            for (int k = 0; k < kItems; k++) {
+                if (code[k] == 1) {
+                    const uint32_t y = ys[k];
+                    queue[nb + rn[k]] = y;
+                    sum_local += off[y + 1] - off[y];
+                } else if (code[k] == 2) {
+                    uint32_t pos = mb + rm[k];
+                    if (pos < kMeetCap) meet[pos] = make_uint2(xs[k], ys[k]);
+                }
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                s.end_q += s.tile_n_tot;
+                s.nmeet = min(s.nmeet + s.tile_m_tot, kMeetCap);
+            }
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) s.vis += G;
+        gbase += G;
+        __syncthreads();
+    }
+    // degree sum of the new level (u32, wrapping like the reference's counter)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        sum_local += __shfl_xor_sync(0xffffffffu, sum_local, o);
+        hits_local += __shfl_xor_sync(0xffffffffu, hits_local, o);
+    }
+    if (threadIdx.x == 0) s.sum_new = 0;
+    __syncthreads();
+    if (lane == 0) {
+        atomicAdd(&s.sum_new, sum_local);
+        atomicAdd(&s.pred_hits, hits_local);
+    }
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(kSamplerBlock, 2) sampler_kernel(SamplerArgs A) {
+    __shared__ SamplerSmem s;
+    const uint32_t slot = blockIdx.x;
+    const uint64_t base = (uint64_t)slot * A.n;
+    NodeRec *rec = A.rec + base;
+    uint32_t *queue = A.queue + base;
+    uint32_t *hits = A.hits + base;
+    uint32_t *touched = A.touched + base;
+    uint2 *meet = A.meet + (uint64_t)slot * kMeetCap;
+    uint64_t *mpre = A.meet_pre + (uint64_t)slot * kMeetCap;
+
+    for (;;) {
+        if (threadIdx.x == 0) s.sample = atomicAdd(A.work_counter, 1u);
+        __syncthreads();
+        const uint32_t sl = s.sample;
+        if (sl >= A.count) break;
+        const uint32_t gidx = A.first_sample + sl;
+
+        // ---- endpoints (Sp_sampler.cpp:46,58-60) and void test (:62-74) -------
+        if (threadIdx.x == 0) {
+            uint32_t d = 0;
+            uint32_t v = draw32(A.seed, gidx, d++) % A.n;
+            uint32_t u = draw32(A.seed, gidx, d++) % A.n;
+            while (u == v) v = draw32(A.seed, gidx, d++) % A.n;
+            s.u = u;
+            s.v = v;
+            s.draw_base = d;
+            s.status = 0;
+            s.vis = 0;
+            s.nmeet = 0;
+            s.ntouched = 0;
+            s.nonmono = 0;
+            s.pred_hits = 0;
+        }
+        __syncthreads();
+        const uint32_t u = s.u, v = s.v;
+        const bool void_cc = A.directed ? (A.cc[u] < A.cc[v]) : (A.cc[u] != A.cc[v]);
+        if (void_cc) {
+            if (threadIdx.x == 0) {
+                A.out_pl[sl] = 0;
+                A.out_np[sl] = 0;
+                A.out_vis[sl] = 0;
+                A.out_status[sl] = 0;
+                A.out_ball[sl] = 0;
+                A.out_pred[sl] = 0;
+            }
+            __syncthreads();
+            continue;
+        }
+        if (threadIdx.x == 0) {
+            rec[u].st = st_make(kSideU, 0);
+            rec[u].sigma = 1;
+            rec[v].st = st_make(kSideV, 0);
+            rec[v].sigma = 1;
+            queue[0] = u;
+            queue[1] = v;
+            s.end_q = 2;
+            s.start_u = 0;
+            s.end_u = 1;
+            s.start_v = 1;
+            s.end_v = 2;
+            s.sum_u = 0;
+            s.sum_v = 0;
+            s.depth_u = 0;
+            s.depth_v = 0;
+        }
+        __syncthreads();
+
+        // ---- balanced bidirectional BFS (:89-144) ------------------------------
+        uint32_t exp_side = kSideU;
+        for (;;) {
+            const bool side_u = s.sum_u <= s.sum_v;
+            exp_side = side_u ? kSideU : kSideV;
+            const uint32_t lo = side_u ? s.start_u : s.start_v;
+            const uint32_t hi = side_u ? s.end_u : s.end_v;
+            const uint32_t depth = side_u ? s.depth_u : s.depth_v;
+            const uint32_t q0 = s.end_q;
+            __syncthreads();
+            expand_level(A, s, rec, queue, meet, exp_side, lo, hi, depth);
+            if (threadIdx.x == 0) {
+                if (side_u) {
+                    s.start_u = q0;
+                    s.end_u = s.end_q;
+                    s.sum_u = s.sum_new;
+                    s.depth_u = depth + 1;
+                } else {
+                    s.start_v = q0;
+                    s.end_v = s.end_q;
+                    s.sum_v = s.sum_new;
+                    s.depth_v = depth + 1;
+                }
+            }
+            __syncthreads();
+            if (s.nmeet > 0 || s.sum_new == 0 || s.status != 0) break;
+        }
+
+        // ---- meeting-edge weights and the number of paths (:159-170) ----------
+        const uint32_t nm = s.nmeet;
+        int32_t np = 0, pl = 0;
+        if (nm > 0 && s.status == 0) {
+            // inclusive prefix of sigma(x) * sigma(y), wrapping; non-decreasing
+            // exactly when the 64-bit sum never wrapped
+            unsigned long long carry = 0;
+            for (uint32_t c0 = 0; c0 < nm; c0 += kSamplerBlock) {
+                uint32_t i = c0 + threadIdx.x;
+                unsigned long long p = 0;
+                if (i < nm) {
+                    uint2 e = __ldcg(&meet[i]);
+                    p = (unsigned long long)__ldcg(&rec[e.x].sigma) *
+                        (unsigned long long)__ldcg(&rec[e.y].sigma);
+                }
+                // block inclusive scan of 64-bit values (wrapping)
+                unsigned long long incl = p;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    unsigned long long t = __shfl_up_sync(0xffffffffu, incl, o);
+                    if ((threadIdx.x & 31) >= o) incl += t;
+                }
+                if ((threadIdx.x & 31) == 31) s.wsum[threadIdx.x >> 5] = incl;
+                __syncthreads();
+                unsigned long long woff = 0;
+                for (int w = 0; w < (int)(threadIdx.x >> 5); w++) woff += s.wsum[w];
+                incl += woff + carry;
+                if (i < nm) mpre[i] = incl;
+                __syncthreads();
+                unsigned long long tot = 0;
+                for (int w = 0; w < kWarps; w++) tot += s.wsum[w];
+                carry += tot;
+                __syncthreads();
+            }
+            __syncthreads();
+            for (uint32_t i = 1 + threadIdx.x; i < nm; i += kSamplerBlock)
+                if (__ldcg(&mpre[i]) < __ldcg(&mpre[i - 1])) s.nonmono = 1;
+            if (threadIdx.x == 0) s.W = carry;
+            __syncthreads();
+            const unsigned long long W = s.W;
+            const uint2 e0 = __ldcg(&meet[0]);
+            const uint32_t L = st_dist(__ldcg(&rec[e0.x].st)) + st_dist(__ldcg(&rec[e0.y].st));
+            if (W == 0ull) {
+                if (threadIdx.x == 0) s.status = SILVAN_E_OVERFLOW;
+            } else {
+                np = 1;
+                if (A.alpha > 0. && W > 1ull) {
+                    double t = A.alpha * (double)W;
+                    np = (t >= 2147483648.0) ? INT32_MIN : (int32_t)t;
+                }
+                pl = np >= 1 ? (int32_t)L : 0;
+                if (pl > 0 && (uint32_t)np > A.np_cap) {
+                    if (threadIdx.x == 0) s.status = SILVAN_E_NP_CAP;
+                } else if (pl > 0 &&
+                           (uint64_t)s.draw_base + (uint64_t)np * (1ull + L) > 0xffffffffull) {
+                    if (threadIdx.x == 0) s.status = SILVAN_E_NP_CAP;
+                }
+            }
+            __syncthreads();
+            // ---- paths (:172-197) and backtracks (:241-265) ------------------
+            if (s.status == 0 && pl > 0) {
+                const bool mono = s.nonmono == 0;
+                for (uint32_t j = threadIdx.x; j < (uint32_t)np; j += kSamplerBlock) {
+                    uint32_t d = s.draw_base + j * (1u + L);
+                    const uint32_t r = (uint32_t)(draw32(A.seed, gidx, d++) % W);
+                    uint32_t ei;
+                    if (mono) {  // first i with prefix > r
+                        uint32_t l = 0, h = nm - 1;
+                        while (l < h) {
+                            uint32_t mid = (l + h) >> 1;
+                            if (__ldcg(&mpre[mid]) > r) h = mid;
+                            else l = mid + 1;
+                        }
+                        ei = l;
+                    } else {
+                        ei = 0;
+                        while (ei < nm && !(__ldcg(&mpre[ei]) > (unsigned long long)r)) ei++;
+                        if (ei >= nm) ei = nm - 1;
+                    }
+                    const uint2 e = __ldcg(&meet[ei]);
+                    uint32_t starts[2] = {e.x, e.y};
+                    for (int h2 = 0; h2 < 2; h2++) {
+                        uint32_t a = starts[h2];
+                        for (uint32_t steps = 0;; steps++) {
+                            // every step moves one level closer to a root, so a
+                            // walk longer than L or an id outside the graph is an
+                            // internal inconsistency: report it, never follow it
+                            if (a >= A.n || steps > L) {
+                                s.status = SILVAN_E_STATE;
+                                break;
+                            }
+                            const uint32_t sta = __ldcg(&rec[a].st);
+                            if (st_dist(sta) == 0) break;  // a is u or v
+                            note_hit(hits, touched, s, a);
+                            const unsigned long long sg = __ldcg(&rec[a].sigma);
+                            uint32_t rr = draw32(A.seed, gidx, d++);
+                            if (sg == 0ull) {
+                                s.status = SILVAN_E_OVERFLOW;
+                                break;
+                            }
+                            rr = (uint32_t)(rr % sg);
+                            const uint32_t c = __ldcg(&rec[a].cnt);
+                            const uint32_t t = min(rr, c - 1u);
+                            if (t == 0) {
+                                a = (uint32_t)__ldcg(
+                                    reinterpret_cast<const unsigned long long *>(&rec[a].first));
+                            } else if (t == c - 1u) {
+                                a = (uint32_t)__ldcg(
+                                    reinterpret_cast<const unsigned long long *>(&rec[a].last));
+                            } else {
+                                a = middle_pred(A, rec, a, sta, t);
+                            }
+                        }
+                    }
+                }
+            }
+            __syncthreads();
+        }
+        if (s.status != 0) {
+            np = 0;
+            pl = 0;
+        }
+
+        // ---- emit the path map, restore the slot ---------------------------------
+        const uint32_t nt = s.ntouched;
+        if (threadIdx.x == 0) {
+            unsigned long long b = 0;
+            if (nt > 0 && s.status == 0) {
+                b = atomicAdd(A.rec_cursor, (unsigned long long)nt);
+                if (b + nt > A.rec_cap) s.status = SILVAN_E_CAPACITY;
+            }
+            s.rec_base = b;
+        }
+        __syncthreads();
+        const unsigned long long rb = s.rec_base;
+        const bool emit = s.status == 0;
+        for (uint32_t i = threadIdx.x; i < nt; i += kSamplerBlock) {
+            const uint32_t a = __ldcg(&touched[i]);
+            if (emit) {
+                PathRec pr;
+                pr.node = a;
+                pr.sample = sl;
+                pr.count = __ldcg(&hits[a]);
+                A.recs[rb + i] = pr;
+            }
+            hits[a] = 0;
+        }
+        const uint32_t eq = s.end_q;
+        for (uint32_t i = threadIdx.x; i < eq; i += kSamplerBlock) rec_reset(&rec[__ldcg(&queue[i])]);
+        if (threadIdx.x == 0) {
+            A.out_pl[sl] = s.status == 0 ? pl : 0;
+            A.out_np[sl] = s.status == 0 ? np : 0;
+            A.out_vis[sl] = s.vis;
+            A.out_status[sl] = s.status;
+            A.out_ball[sl] = s.end_q;
+            A.out_pred[sl] = s.pred_hits;
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void init_slots_kernel(NodeRec *rec, uint32_t *hits, uint64_t total) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < total;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        rec_reset(&rec[i]);
+        hits[i] = 0;
+    }
+}
+
+}  // namespace
+
+cudaError_t sampler_init_slots(NodeRec *rec, uint32_t *hits, uint64_t total_nodes,
+                               cudaStream_t stream) {
+    init_slots_kernel<<<1184, 256, 0, stream>>>(rec, hits, total_nodes);
+    return cudaGetLastError();
+}
+
+cudaError_t sampler_launch(const SamplerArgs &a, uint32_t grid, cudaStream_t stream) {
+    if (grid == 0) return cudaSuccess;
+    sampler_kernel<<<grid, kSamplerBlock, 0, stream>>>(a);
+    return cudaGetLastError();
+}
+
+int sampler_max_ctas_per_sm() {
+    int n = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, sampler_kernel, kSamplerBlock, 0);
+    return n;
+}
+
+}  // namespace silvan

@@ -1,0 +1,99 @@
+"""The CPU oracle, pinned: Philox known answers, the committed golden
+fixtures (outputs of the reference's own sources with the same stream) and,
+where the reference build is present, fresh random cases against it."""
+import ctypes as C
+import json
+import os
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+with open(os.path.join(GOLDEN, "manifest.json")) as f:
+    MANIFEST = json.load(f)
+
+
+def golden(name):
+    return dict(np.load(os.path.join(GOLDEN, name + ".npz")))
+
+
+def test_philox_known_answers(port):
+    # Known-answer vectors of Philox4x32-10 from the Random123 distribution
+    # (kat_vectors): zero counter/key, all-ones counter/key, digits of pi.
+    f = port.lib.orc_philox4x32
+    f.argtypes = [C.c_void_p] * 3
+    cases = [
+        ([0, 0, 0, 0], [0, 0], [0x6627e8d5, 0xe169c58d, 0xbc57ac4c, 0x9b00dbd8]),
+        ([0xffffffff] * 4, [0xffffffff] * 2, [0x408f276d, 0x41c83b0e, 0xa20bc7c6, 0x6d5451fd]),
+        ([0x243f6a88, 0x85a308d3, 0x13198a2e, 0x03707344], [0xa4093822, 0x299f31d0],
+         [0xd16cfe09, 0x94fdcceb, 0x5001e420, 0x24126ea1]),
+    ]
+    for ctr, key, want in cases:
+        c = np.array(ctr, np.uint32)
+        k = np.array(key, np.uint32)
+        o = np.zeros(4, np.uint32)
+        f(c.ctypes.data, k.ctypes.data, o.ctypes.data)
+        assert o.tolist() == want
+
+
+def golden_port_graph(port, g, directed):
+    return port.graph(int(g["n"]), directed, g["out_off"], g["out_adj"], g["in_off"], g["in_adj"],
+                      g["cc"])
+
+
+@pytest.mark.parametrize("name", [k for k in MANIFEST if "_" not in k])
+@pytest.mark.parametrize("alpha,tag", [(2.3, "a23"), (-1.0, "am1")])
+def test_port_replay_matches_golden(port, name, alpha, tag):
+    m = MANIFEST[name]
+    g = golden(name)
+    pg = golden_port_graph(port, g, m["directed"])
+    r = pg.replay(m["seed"], 0, m["replay"], alpha)
+    for f in ("path_length", "num_paths", "vis_edges", "offsets", "nodes", "counts"):
+        np.testing.assert_array_equal(getattr(r, f), g[f"{tag}_{f}"], err_msg=f)
+
+
+@pytest.mark.parametrize("name", sorted(MANIFEST))
+def test_port_run_matches_golden(port, name):
+    m = MANIFEST[name]
+    g = golden(name)
+    pg = golden_port_graph(port, g, m["directed"])
+    run = dict(m["run"])
+    o = pg.run(int(g["diameter"]), run.pop("eps"), run.pop("delta"), seed=m["seed"], **run)
+    for f in ("approx", "wimpy", "mcrade", "partition_index", "ranking_elements",
+              "ranking_values", "sp_lengths", "epsilon_partition", "partition_ids"):
+        np.testing.assert_array_equal(o[f], g["run_" + f], err_msg=f)
+    for f, v in m["scalars"].items():
+        assert o[f] == v, f
+
+
+@pytest.fixture(scope="module")
+def ref():
+    from oracle.oracle import Ref, ref_available
+    if not ref_available():
+        pytest.skip("reference build not present")
+    return Ref()
+
+
+@pytest.mark.parametrize("seed", [3, 77, 2**33 + 5])
+def test_port_matches_reference_sources(ref, port, sb, tmp_path, seed):
+    # fresh graphs and seeds, both sampling modes, against the reference's code
+    for kind, kw, directed in [("rmat", (10, 6, seed % 97, True), True),
+                               ("ba", (800, 2, seed % 89), False)]:
+        pairs = sb.rmat(*kw) if kind == "rmat" else sb.barabasi_albert(*kw)
+        path = str(tmp_path / f"{kind}.txt")
+        sb.write_edge_list(path, pairs)
+        rg = ref.graph(path, directed)
+        D, cc, nc = rg.diameter()
+        oo, oa, io, ia = rg.csr()
+        pg = port.graph(rg.n, directed, oo, oa, io, ia, cc)
+        for alpha in (2.3, -1.0):
+            a = rg.replay(seed, 1000, 400, alpha)
+            b = pg.replay(seed, 1000, 400, alpha)
+            for f in ("path_length", "num_paths", "vis_edges", "offsets", "nodes", "counts"):
+                np.testing.assert_array_equal(getattr(a, f), getattr(b, f))
+        ra = ref.run(path, directed, 0.05, 0.1, seed=seed)
+        rb = pg.run(D, 0.05, 0.1, seed=seed)
+        for f in ("approx", "wimpy", "mcrade", "partition_index"):
+            np.testing.assert_array_equal(ra[f], rb[f])
