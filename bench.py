@@ -194,6 +194,10 @@ def main():
     ap.add_argument("--config", default="rmat20", choices=sorted(CONFIGS))
     ap.add_argument("--form", default="batched", choices=["batched", "plain"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--slots", type=int, default=0,
+                    help="sampler slots (0 = occupancy x SMs); small values bound the device "
+                         "memory for profiler captures")
     args = ap.parse_args()
     cfg = CONFIGS[args.config]
     if args.impl == "reference":
@@ -219,7 +223,7 @@ def main():
 
     def one_run(seed):
         job = sb.Probabilistic(g, cfg["eps"], cfg["delta"], k=cfg["k"], seed=seed,
-                               form=args.form)
+                               form=args.form, slots=args.slots)
         res = job.run()
         del job
         return res
@@ -247,12 +251,12 @@ def main():
     if csr.directed:
         h2d += int(csr.in_off.nbytes // 2 + csr.in_adj.nbytes)
     d2h = csr.n * 8
-    for s in range(args.steps):
+    for s in range(0 if args.no_e2e else args.steps):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         g2 = sb.Graph.upload(csr, with_cc=True)
         job = sb.Probabilistic(g2, cfg["eps"], cfg["delta"], k=cfg["k"],
-                               seed=seed0 + 50 + s, form=args.form)
+                               seed=seed0 + 50 + s, form=args.form, slots=args.slots)
         r = job.run()
         est = job.get_centrality()
         torch.cuda.synchronize()
@@ -312,11 +316,21 @@ def main():
             "samples_per_step": samples_all / max(1, world) / args.steps,
             "backtracked_paths_per_step": sum(r["backtracked_paths"] for r in results) /
                                           args.steps,
-            "e2e": {"value": e2e_s_all / e2e_t_max, "unit": "paths/s",
+            "e2e": {"value": e2e_s_all / e2e_t_max if e2e_t_max > 0 else None,
+                    "unit": "paths/s",
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "kernel": "sampler_kernel", "peak_kind": peak_kind},
+            "breakdown_ms_per_step": {
+                "sampler": 1000 * sum(r["time_sampling_s"] for r in results) / args.steps,
+                "commit": 1000 * sum(r["time_apply_s"] for r in results) / args.steps,
+                "total": 1000 * t_dev / args.steps},
+            "work_per_step": {
+                "vis_edges": sum(r["vis_edges"] for r in results) / args.steps,
+                "ball_nodes": sum(r["ball_nodes"] for r in results) / args.steps,
+                "pred_entries": sum(r["pred_entries"] for r in results) / args.steps,
+                "checks": sum(r["checks"] for r in results) / args.steps},
             "cpu_baseline": cpu,
             "gpu_launches": launches,
             "clocks": clk.summary(),

@@ -186,17 +186,82 @@ int silvan_job_destroy(silvan_job_t j);
 /* Progress of the sampling loop. */
 typedef struct {
     uint64_t samples;       /* samples committed in the current pass        */
-    uint64_t void_samples;
-    uint64_t vis_edges;
+    uint64_t void_samples;  /* void samples of the current pass              */
+    uint64_t vis_edges;     /* edges visited in the current pass             */
     uint64_t backtracked_paths;
     int32_t pass;           /* 1 or 2                                       */
-    int32_t error;          /* first device status (SILVAN_E_*) or 0       */
+    int32_t done;           /* 1 once the stopping rule has fired           */
 } silvan_status_t;
 
-/* Draws and commits samples of the current pass until `target` samples
- * have been committed (one Probabilistic::one_round per sample,
- * silvan/src/Probabilistic.cpp:468-559). */
-int silvan_run_rounds(silvan_job_t j, uint64_t target, silvan_status_t *st);
+/* Advances the estimator by at most `rounds` rounds of its own schedule.  A
+ * round draws the samples up to the next point at which the reference acts
+ * (the end of pass 1, a stopping-rule evaluation, the omega cap; every
+ * 11-sample block in the plain form), commits them in sample order
+ * (Probabilistic::one_round, silvan/src/Probabilistic.cpp:468-559) and
+ * evaluates that point.  The first call starts the run; results are read
+ * with silvan_job_result once status.done is set. */
+int silvan_run_rounds(silvan_job_t j, uint32_t rounds, silvan_status_t *st, void *log);
+
+/* Result of a finished job (after silvan_job_run or the last round). */
+int silvan_job_result(silvan_job_t j, silvan_result_t *res);
+
+/* ---- multi-graph batching ------------------------------------------------- */
+
+/* Runs `count` jobs (on the same or different graphs) to completion with one
+ * persistent sampler launch per round serving every unfinished job, each job
+ * following its own schedule (no counterpart in the reference, which runs one
+ * graph per process).  Sampler slots are sized for the largest graph; they
+ * take at most mem_budget bytes (0 = half of the free device memory).
+ * results[i] receives job i's result.  Each job's estimates are the same as
+ * when it runs alone. */
+int silvan_jobs_run_batched(silvan_job_t *jobs, uint32_t count, uint64_t mem_budget,
+                            silvan_result_t *results, void *log);
+
+/* ---- serving ---------------------------------------------------------------
+ * An estimation server with continuous batching (no counterpart in the
+ * reference, which runs one estimation per process).  Requests are submitted
+ * from any thread; one server thread owns the device, admits queued requests
+ * in arrival order while their device memory fits the budget, keeps their
+ * graphs and sampler state on the device, and serves every active request in
+ * each round's single persistent sampler launch.  A request's result is the
+ * same as when it runs alone. */
+typedef struct silvan_server_s *silvan_server_t;
+
+#define SILVAN_REQ_QUEUED 1
+#define SILVAN_REQ_RUNNING 2
+#define SILVAN_REQ_DONE 3   /* negative values: the request failed (SILVAN_E_*) */
+
+typedef struct {
+    uint64_t rounds;        /* sampler rounds run                             */
+    uint64_t samples;       /* samples drawn over all requests                */
+    uint64_t max_active;    /* most requests served by one round              */
+    uint64_t queued, active;
+    uint64_t bytes_in_use;  /* device bytes held by admitted requests        */
+    uint64_t budget;        /* admission budget                               */
+    uint32_t slots;         /* sampler slots                                  */
+    uint32_t pad;
+} silvan_server_stats_t;
+
+/* n_max: largest graph (nodes) the server accepts; the sampler slots are
+ * sized for it.  budget: device bytes for admitted requests (0 = a third of
+ * the free memory).  slots: 0 = occupancy x SM count. */
+int silvan_server_create(uint64_t n_max, uint64_t budget, uint32_t slots, silvan_server_t *out);
+/* Queues an estimation of graph g (copied; g may be destroyed afterwards). */
+int silvan_server_submit(silvan_server_t s, silvan_host_graph_t g, const silvan_params_t *p,
+                         uint64_t *id);
+/* state: SILVAN_REQ_*; once done, res, the latency from submission to the
+ * result and the time spent queued are filled. */
+int silvan_server_poll(silvan_server_t s, uint64_t id, int32_t *state, silvan_result_t *res,
+                       double *latency_s, double *queued_s);
+/* Blocks until the request finished or timeout_s passed (SILVAN_E_TIMEOUT). */
+int silvan_server_wait(silvan_server_t s, uint64_t id, double timeout_s);
+/* Estimates (approx / num_samples, n entries) and, in top-k mode, the ranked
+ * output of a finished request.  Any pointer may be NULL. */
+int silvan_server_estimates(silvan_server_t s, uint64_t id, double *out, uint32_t n,
+                            uint32_t *topk_nodes, double *topk_values, uint32_t topk_cap,
+                            uint32_t *topk_count);
+int silvan_server_stats(silvan_server_t s, silvan_server_stats_t *st);
+int silvan_server_destroy(silvan_server_t s);
 
 /* ---- per-sample replay (parity hook) -------------------------------------- */
 

@@ -33,8 +33,13 @@ EXPORTS = [
     "silvan_host_graph_destroy", "silvan_graph_from_host", "silvan_job_create",
     "silvan_job_run", "silvan_read_estimates", "silvan_read_topk", "silvan_read_counters",
     "silvan_job_destroy", "silvan_run_rounds", "silvan_replay_samples", "silvan_generate",
-    "silvan_graph_from_pairs", "silvan_last_error", "silvan_version",
+    "silvan_graph_from_pairs", "silvan_last_error", "silvan_version", "silvan_job_result",
+    "silvan_jobs_run_batched", "silvan_server_create", "silvan_server_submit",
+    "silvan_server_poll", "silvan_server_wait", "silvan_server_estimates", "silvan_server_stats",
+    "silvan_server_destroy",
 ]
+
+REQ_QUEUED, REQ_RUNNING, REQ_DONE = 1, 2, 3
 
 
 class SilvanError(RuntimeError):
@@ -79,7 +84,7 @@ class Result(C.Structure):
 
 class Status(C.Structure):
     _fields_ = [("samples", C.c_uint64), ("void_samples", C.c_uint64), ("vis_edges", C.c_uint64),
-                ("backtracked_paths", C.c_uint64), ("pass_", C.c_int32), ("error", C.c_int32)]
+                ("backtracked_paths", C.c_uint64), ("pass_", C.c_int32), ("done", C.c_int32)]
 
 
 _lib = None
@@ -111,7 +116,9 @@ def load(path: str = LIB_PATH):
         "silvan_graph_from_pairs": (C.c_int, [P, C.c_uint64, C.c_int, P]),
         "silvan_job_create": (C.c_int, [P, P, P]),
         "silvan_job_run": (C.c_int, [P, P, P]),
-        "silvan_run_rounds": (C.c_int, [P, C.c_uint64, P]),
+        "silvan_run_rounds": (C.c_int, [P, C.c_uint32, P, P]),
+        "silvan_job_result": (C.c_int, [P, P]),
+        "silvan_jobs_run_batched": (C.c_int, [P, C.c_uint32, C.c_uint64, P, P]),
         "silvan_read_estimates": (C.c_int, [P, P, C.c_uint32]),
         "silvan_read_topk": (C.c_int, [P, P, P, C.c_uint32, P]),
         "silvan_read_counters": (C.c_int, [P, P, P, P, P]),
@@ -120,6 +127,13 @@ def load(path: str = LIB_PATH):
                                             C.c_uint32, P, P, P, P, P, P, P, C.c_uint64, P]),
         "silvan_generate": (C.c_int, [C.c_int, C.c_uint32, C.c_uint32, C.c_uint32, C.c_double,
                                       C.c_double, C.c_uint64, P, C.c_uint64, P]),
+        "silvan_server_create": (C.c_int, [C.c_uint64, C.c_uint64, C.c_uint32, P]),
+        "silvan_server_submit": (C.c_int, [P, P, P, P]),
+        "silvan_server_poll": (C.c_int, [P, C.c_uint64, P, P, P, P]),
+        "silvan_server_wait": (C.c_int, [P, C.c_uint64, C.c_double]),
+        "silvan_server_estimates": (C.c_int, [P, C.c_uint64, P, C.c_uint32, P, P, C.c_uint32, P]),
+        "silvan_server_stats": (C.c_int, [P, P]),
+        "silvan_server_destroy": (C.c_int, [P]),
         "silvan_last_error": (C.c_char_p, []),
         "silvan_version": (C.c_char_p, []),
     }
@@ -383,6 +397,17 @@ class Probabilistic:
         self.result = res.as_dict()
         return self.result
 
+    def step(self, rounds=1):
+        """Runs at most `rounds` rounds of the job's own schedule (silvan_run_rounds)."""
+        st = Status()
+        _check(load().silvan_run_rounds(self.h, rounds, C.byref(st), None))
+        d = {f: getattr(st, f) for f, _ in Status._fields_}
+        if st.done:
+            res = Result()
+            _check(load().silvan_job_result(self.h, C.byref(res)))
+            self.result = res.as_dict()
+        return d
+
     def get_centrality(self):
         """approx[v] / num_samples for every node."""
         n = self.graph.n
@@ -412,5 +437,86 @@ class Probabilistic:
         try:
             if getattr(self, "h", None):
                 load().silvan_job_destroy(self.h)
+        except Exception:
+            pass
+
+
+def run_batched(jobs, mem_budget=0):
+    """Runs several jobs (same or different graphs) to completion with one
+    persistent sampler launch per round for all unfinished jobs; returns each
+    job's result dict (silvan_jobs_run_batched)."""
+    lib = load()
+    n = len(jobs)
+    handles = (C.c_void_p * n)(*[j.h.value if isinstance(j.h, C.c_void_p) else j.h for j in jobs])
+    res = (Result * n)()
+    _check(lib.silvan_jobs_run_batched(handles, n, mem_budget, res, None))
+    out = []
+    for j, r in zip(jobs, res):
+        j.result = r.as_dict()
+        out.append(j.result)
+    return out
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("rounds", C.c_uint64), ("samples", C.c_uint64), ("max_active", C.c_uint64),
+                ("queued", C.c_uint64), ("active", C.c_uint64), ("bytes_in_use", C.c_uint64),
+                ("budget", C.c_uint64), ("slots", C.c_uint32), ("pad", C.c_uint32)]
+
+
+class Server:
+    """Estimation server with continuous batching (silvan_server_*): requests
+    on graphs of different sizes are admitted by device-memory budget and
+    served together, one persistent sampler launch per round."""
+
+    def __init__(self, n_max, budget=0, slots=0):
+        h = C.c_void_p()
+        _check(load().silvan_server_create(n_max, budget, slots, C.byref(h)))
+        self.h = h
+
+    def submit(self, hg: HostGraph, eps, delta, k=0, alpha=2.3, alpha_given=False, a=2.0,
+               m_hat=True, seed=42, np_cap=0):
+        lib = load()
+        p = Params()
+        lib.silvan_params_default(C.byref(p))
+        p.eps, p.delta, p.k = eps, delta, k
+        p.alpha, p.alpha_given, p.a = alpha, int(alpha_given), a
+        p.m_hat, p.seed, p.np_cap = int(m_hat), seed, np_cap
+        rid = C.c_uint64()
+        _check(lib.silvan_server_submit(self.h, hg.h, C.byref(p), C.byref(rid)))
+        return rid.value
+
+    def poll(self, rid):
+        st = C.c_int32()
+        res = Result()
+        lat = C.c_double()
+        qd = C.c_double()
+        _check(load().silvan_server_poll(self.h, rid, C.byref(st), C.byref(res), C.byref(lat),
+                                         C.byref(qd)))
+        if st.value == REQ_DONE:
+            return st.value, dict(res.as_dict(), latency_s=lat.value, queued_s=qd.value)
+        return st.value, None
+
+    def wait(self, rid, timeout_s=600.0):
+        _check(load().silvan_server_wait(self.h, rid, timeout_s))
+        return self.poll(rid)[1]
+
+    def estimates(self, rid, n):
+        out = np.zeros(n, np.float64)
+        _check(load().silvan_server_estimates(self.h, rid, _p(out), n, None, None, 0, None))
+        return out
+
+    def stats(self):
+        s = ServerStats()
+        _check(load().silvan_server_stats(self.h, C.byref(s)))
+        return {f: getattr(s, f) for f, _ in ServerStats._fields_}
+
+    def close(self):
+        if getattr(self, "h", None):
+            load().silvan_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
         except Exception:
             pass

@@ -7,6 +7,7 @@
 
 #include "engine.h"
 #include "gen.h"
+#include "server.h"
 #include "silvan.h"
 
 namespace silvan {
@@ -21,6 +22,9 @@ struct silvan_host_graph_s {
     std::vector<uint32_t> cc;
     uint32_t ncomp = 0, diameter = 0;
     double seconds = 0;
+};
+struct silvan_server_s {
+    silvan::Server *s;
 };
 struct silvan_job_s {
     silvan::Job *job;
@@ -337,12 +341,37 @@ int silvan_job_run(silvan_job_t j, silvan_result_t *res, void *log) {
     return j->job->run(res, (FILE *)log);
 }
 
-int silvan_run_rounds(silvan_job_t j, uint64_t target, silvan_status_t *st) {
+int silvan_run_rounds(silvan_job_t j, uint32_t rounds, silvan_status_t *st, void *log) {
     if (!j) {
         set_error("null argument");
         return SILVAN_E_BADARG;
     }
-    return j->job->run_to(target, st);
+    return j->job->step(rounds, st, (FILE *)log);
+}
+
+int silvan_job_result(silvan_job_t j, silvan_result_t *res) {
+    if (!j || !res) {
+        set_error("null argument");
+        return SILVAN_E_BADARG;
+    }
+    return j->job->finish(res);
+}
+
+int silvan_jobs_run_batched(silvan_job_t *jobs, uint32_t count, uint64_t mem_budget,
+                            silvan_result_t *results, void *log) {
+    if ((!jobs && count) || (!results && count)) {
+        set_error("null argument");
+        return SILVAN_E_BADARG;
+    }
+    std::vector<Job *> js(count);
+    for (uint32_t i = 0; i < count; i++) {
+        if (!jobs[i]) {
+            set_error("null job");
+            return SILVAN_E_BADARG;
+        }
+        js[i] = jobs[i]->job;
+    }
+    return run_batched(js, mem_budget, results, (FILE *)log);
 }
 
 int silvan_read_estimates(silvan_job_t j, double *out, uint32_t n) {
@@ -375,6 +404,71 @@ int silvan_job_destroy(silvan_job_t j) {
     if (!j) return SILVAN_OK;
     delete j->job;
     delete j;
+    return SILVAN_OK;
+}
+
+int silvan_server_create(uint64_t n_max, uint64_t budget, uint32_t slots, silvan_server_t *out) {
+    if (!out || n_max < 2) {
+        set_error("bad argument");
+        return SILVAN_E_BADARG;
+    }
+    int rc = check_device();
+    if (rc) return rc;
+    Server *s = nullptr;
+    rc = server_create(n_max, budget, slots, &s);
+    if (rc != SILVAN_OK) return rc;
+    *out = new silvan_server_s{s};
+    return SILVAN_OK;
+}
+
+int silvan_server_submit(silvan_server_t s, silvan_host_graph_t g, const silvan_params_t *p,
+                         uint64_t *id) {
+    if (!s || !g || !p || !id) {
+        set_error("null argument");
+        return SILVAN_E_BADARG;
+    }
+    return server_submit(s->s, g->host, g->cc, g->ncomp, g->diameter, *p, id);
+}
+
+int silvan_server_poll(silvan_server_t s, uint64_t id, int32_t *state, silvan_result_t *res,
+                       double *latency_s, double *queued_s) {
+    if (!s) {
+        set_error("null argument");
+        return SILVAN_E_BADARG;
+    }
+    return server_poll(s->s, id, state, res, latency_s, queued_s);
+}
+
+int silvan_server_wait(silvan_server_t s, uint64_t id, double timeout_s) {
+    if (!s) {
+        set_error("null argument");
+        return SILVAN_E_BADARG;
+    }
+    return server_wait(s->s, id, timeout_s);
+}
+
+int silvan_server_estimates(silvan_server_t s, uint64_t id, double *out, uint32_t n,
+                            uint32_t *topk_nodes, double *topk_values, uint32_t topk_cap,
+                            uint32_t *topk_count) {
+    if (!s) {
+        set_error("null argument");
+        return SILVAN_E_BADARG;
+    }
+    return server_estimates(s->s, id, out, n, topk_nodes, topk_values, topk_cap, topk_count);
+}
+
+int silvan_server_stats(silvan_server_t s, silvan_server_stats_t *st) {
+    if (!s || !st) {
+        set_error("null argument");
+        return SILVAN_E_BADARG;
+    }
+    return server_stats(s->s, st);
+}
+
+int silvan_server_destroy(silvan_server_t s) {
+    if (!s) return SILVAN_OK;
+    server_destroy(s->s);
+    delete s;
     return SILVAN_OK;
 }
 

@@ -23,19 +23,23 @@ namespace {
 constexpr int kScanBlocks = 296;
 constexpr int kScanThreads = 256;
 
-__device__ __forceinline__ uint32_t round_records(const RoundBuffers &rb) {
-    unsigned long long c = *rb.rec_cursor;
-    return (uint32_t)(c < rb.rec_cap ? c : rb.rec_cap);
+__device__ __forceinline__ uint32_t round_records(const RoundBuffers &rb, const ApplyArgs &a) {
+    return (uint32_t)min((uint64_t)a.n_records, rb.rec_cap);
 }
 
-__global__ void signs_kernel(RoundBuffers rb, ApplyArgs a) {
+__global__ void signs_kernel(const ApplyState *st) {
+    const RoundBuffers rb = st->rb;
+    const ApplyArgs a = st->a;
+    if (a.pass != 2) return;
     for (uint32_t s = a.lo + blockIdx.x * blockDim.x + threadIdx.x; s < a.hi;
          s += gridDim.x * blockDim.x)
         rb.signs[s] = rademacher_mask(a.seed, a.first_sample + s);
 }
 
-__global__ void bucket_count_kernel(RoundBuffers rb, ApplyArgs a) {
-    const uint32_t R = round_records(rb);
+__global__ void bucket_count_kernel(const ApplyState *st) {
+    const RoundBuffers rb = st->rb;
+    const ApplyArgs a = st->a;
+    const uint32_t R = round_records(rb, a);
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < R; i += gridDim.x * blockDim.x) {
         PathRec r = rb.recs[i];
         if (r.sample < a.lo || r.sample >= a.hi) continue;
@@ -69,8 +73,9 @@ __device__ uint32_t block_sum(uint32_t v, uint32_t *tmp) {
     return t;
 }
 
-__global__ void scan_reduce_kernel(RoundBuffers rb) {
+__global__ void scan_reduce_kernel(const ApplyState *st) {
     __shared__ uint32_t tmp[32];
+    const RoundBuffers rb = st->rb;
     const uint32_t T = *rb.n_touched;
     uint32_t b, e;
     range_of(T, b, e);
@@ -80,7 +85,8 @@ __global__ void scan_reduce_kernel(RoundBuffers rb) {
     if (threadIdx.x == 0) rb.block_sums[blockIdx.x] = s;
 }
 
-__global__ void scan_top_kernel(RoundBuffers rb, int nblocks) {
+__global__ void scan_top_kernel(const ApplyState *st, int nblocks) {
+    const RoundBuffers rb = st->rb;
     if (threadIdx.x == 0 && blockIdx.x == 0) {
         uint32_t acc = 0;
         for (int i = 0; i < nblocks; i++) {
@@ -92,8 +98,9 @@ __global__ void scan_top_kernel(RoundBuffers rb, int nblocks) {
     }
 }
 
-__global__ void scan_down_kernel(RoundBuffers rb) {
+__global__ void scan_down_kernel(const ApplyState *st) {
     __shared__ uint32_t tmp[33];
+    const RoundBuffers rb = st->rb;
     const uint32_t T = *rb.n_touched;
     uint32_t b, e;
     range_of(T, b, e);
@@ -134,8 +141,10 @@ __global__ void scan_down_kernel(RoundBuffers rb) {
     if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) rb.bucket_off[T] = rb.block_sums[gridDim.x];
 }
 
-__global__ void bucket_scatter_kernel(RoundBuffers rb, ApplyArgs a) {
-    const uint32_t R = round_records(rb);
+__global__ void bucket_scatter_kernel(const ApplyState *st) {
+    const RoundBuffers rb = st->rb;
+    const ApplyArgs a = st->a;
+    const uint32_t R = round_records(rb, a);
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < R; i += gridDim.x * blockDim.x) {
         PathRec r = rb.recs[i];
         if (r.sample < a.lo || r.sample >= a.hi) continue;
@@ -150,56 +159,83 @@ __device__ __forceinline__ void atomic_max_nonneg_double(unsigned long long *p, 
 
 // Sequential fold of one node's sorted contributions.  Lane j < 25 carries
 // trial j of mcrade, lane 25 approx (and the top-k mark), lane 26 the wimpy
-// variance.  get(r) returns the r-th (sample << 32 | count) entry.
+// variance.  get(r) returns the r-th (sample << 32 | count) entry.  Entries
+// are prepared 32 at a time by all lanes (x = count * (1/num_paths) and the
+// sample's signs, into the warp's shared scratch) so that the sequential
+// chains only read shared memory.
+struct FoldScratch {
+    double x[32];
+    uint32_t signs[32];
+    uint32_t sample[32];
+};
+
 template <typename Get>
 __device__ void fold_node(const RoundBuffers &rb, const JobCounters &jc, const ApplyArgs &a,
-                          uint32_t node, uint32_t b, Get get) {
+                          uint32_t node, uint32_t b, Get get, FoldScratch &fs) {
     const int lane = threadIdx.x & 31;
+    const bool pass2 = a.pass == 2;
+    long long m = 0;
+    double acc = 0.0;
+    uint32_t lu = 0;
     if (lane < kTrials) {
-        if (a.pass != 2) return;
-        long long *mp = &jc.mcrade[(uint64_t)node * kTrials + lane];
-        long long m = *mp;
-        for (uint32_t r = 0; r < b; r++) {
-            const unsigned long long e = get(r);
-            const uint32_t sl = (uint32_t)(e >> 32);
-            const uint32_t c = (uint32_t)e;
-            const double x = __dmul_rn((double)c, __ddiv_rn(1.0, (double)rb.np[sl]));
-            const bool plus = (rb.signs[sl] >> lane) & 1u;
-            m = (long long)__double2ll_rz(__dadd_rn(__ll2double_rn(m), plus ? x : -x));
-        }
-        *mp = m;
+        if (pass2) m = jc.mcrade[(uint64_t)node * kTrials + lane];
     } else if (lane == 25) {
-        double ap = jc.approx[node];
-        uint32_t lu = 0;
-        for (uint32_t r = 0; r < b; r++) {
+        acc = jc.approx[node];
+    } else if (lane == 26) {
+        acc = jc.wimpy[node];
+    }
+    bool crossed = a.track_cross ? jc.cross_flag[node] != 0 : true;
+    for (uint32_t r0 = 0; r0 < b; r0 += 32) {
+        const uint32_t r = r0 + lane;
+        if (r < b) {
             const unsigned long long e = get(r);
             const uint32_t sl = (uint32_t)(e >> 32);
             const uint32_t c = (uint32_t)e;
-            const double x = __dmul_rn((double)c, __ddiv_rn(1.0, (double)rb.np[sl]));
-            if (x > 0.) {
-                ap = __dadd_rn(ap, x);
-                lu = a.first_sample + sl + 1u;
-                if (a.track_cross && !jc.cross_flag[node] && ap >= 3.0) {
-                    jc.cross_flag[node] = 1;
-                    uint32_t k = atomicAdd(&jc.sc->n_cross, 1u);
-                    jc.cross_sample[k] = a.first_sample + sl;
+            fs.x[lane] = __dmul_rn((double)c, __ddiv_rn(1.0, (double)rb.np[sl]));
+            fs.signs[lane] = pass2 ? rb.signs[sl] : 0u;
+            fs.sample[lane] = sl;
+        }
+        __syncwarp();
+        const uint32_t kmax = min(32u, b - r0);
+        if (lane < kTrials) {
+            if (pass2) {
+                for (uint32_t k = 0; k < kmax; k++) {
+                    const double x = fs.x[k];
+                    const bool plus = (fs.signs[k] >> lane) & 1u;
+                    m = (long long)__double2ll_rz(__dadd_rn(__ll2double_rn(m), plus ? x : -x));
                 }
             }
+        } else if (lane == 25) {
+            for (uint32_t k = 0; k < kmax; k++) {
+                const double x = fs.x[k];
+                if (x > 0.) {
+                    acc = __dadd_rn(acc, x);
+                    lu = a.first_sample + fs.sample[k] + 1u;
+                    if (!crossed && acc >= 3.0) {
+                        crossed = true;
+                        jc.cross_flag[node] = 1;
+                        const uint32_t q = atomicAdd(&jc.sc->n_cross, 1u);
+                        jc.cross_sample[q] = a.first_sample + fs.sample[k];
+                    }
+                }
+            }
+        } else if (lane == 26) {
+            for (uint32_t k = 0; k < kmax; k++) {
+                const double x = fs.x[k];
+                if (x > 0.) acc = __dadd_rn(acc, __dmul_rn(x, x));
+            }
         }
-        jc.approx[node] = ap;
+        __syncwarp();
+    }
+    if (lane < kTrials) {
+        if (pass2) jc.mcrade[(uint64_t)node * kTrials + lane] = m;
+    } else if (lane == 25) {
+        jc.approx[node] = acc;
         if (lu) jc.last_upd[node] = lu;
-        atomic_max_nonneg_double(&jc.sc->sup_approx_bits, ap);
+        atomic_max_nonneg_double(&jc.sc->sup_approx_bits, acc);
     } else if (lane == 26) {
-        double w = jc.wimpy[node];
-        for (uint32_t r = 0; r < b; r++) {
-            const unsigned long long e = get(r);
-            const uint32_t sl = (uint32_t)(e >> 32);
-            const uint32_t c = (uint32_t)e;
-            const double x = __dmul_rn((double)c, __ddiv_rn(1.0, (double)rb.np[sl]));
-            if (x > 0.) w = __dadd_rn(w, __dmul_rn(x, x));
-        }
-        jc.wimpy[node] = w;
-        atomic_max_nonneg_double(&jc.sc->sup_wimpy_bits, w);
+        jc.wimpy[node] = acc;
+        atomic_max_nonneg_double(&jc.sc->sup_wimpy_bits, acc);
     }
 }
 
@@ -219,9 +255,12 @@ __device__ __forceinline__ void warp_bitonic_sort(unsigned long long &key) {
 constexpr int kApplyThreads = 256;
 
 // Groups of at most 32 entries: one warp per node.
-__global__ void __launch_bounds__(kApplyThreads) apply_small_kernel(RoundBuffers rb, JobCounters jc,
-                                                                     ApplyArgs a) {
+__global__ void __launch_bounds__(kApplyThreads) apply_small_kernel(const ApplyState *st) {
     __shared__ unsigned long long buf[kApplyThreads / 32][32];
+    __shared__ FoldScratch fsc[kApplyThreads / 32];
+    const RoundBuffers rb = st->rb;
+    const JobCounters jc = st->jc;
+    const ApplyArgs a = st->a;
     const uint32_t T = *rb.n_touched;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const uint32_t gw = blockIdx.x * (blockDim.x >> 5) + wib;
@@ -235,16 +274,19 @@ __global__ void __launch_bounds__(kApplyThreads) apply_small_kernel(RoundBuffers
         warp_bitonic_sort(key);
         buf[wib][lane] = key;
         __syncwarp();
-        fold_node(rb, jc, a, node, b, [&](uint32_t r) { return buf[wib][r]; });
+        fold_node(rb, jc, a, node, b, [&](uint32_t r) { return buf[wib][r]; }, fsc[wib]);
         __syncwarp();
     }
 }
 
 // Groups of more than 32 entries: one CTA per node, bitonic sort in shared
 // memory (groups are bounded by kLargeBucket through the sub-round size).
-__global__ void __launch_bounds__(1024) apply_large_kernel(RoundBuffers rb, JobCounters jc,
-                                                           ApplyArgs a) {
+__global__ void __launch_bounds__(1024) apply_large_kernel(const ApplyState *st) {
     extern __shared__ unsigned long long sbuf[];
+    __shared__ FoldScratch fsc;
+    const RoundBuffers rb = st->rb;
+    const JobCounters jc = st->jc;
+    const ApplyArgs a = st->a;
     const uint32_t T = *rb.n_touched;
     for (uint32_t t = blockIdx.x; t < T; t += gridDim.x) {
         const uint32_t b0 = rb.bucket_off[t];
@@ -277,13 +319,16 @@ __global__ void __launch_bounds__(1024) apply_large_kernel(RoundBuffers rb, JobC
         }
         if (threadIdx.x < 32) {
             const uint32_t node = rb.touched[t];
-            fold_node(rb, jc, a, node, b, [&](uint32_t r) { return sbuf[r]; });
+            fold_node(rb, jc, a, node, b, [&](uint32_t r) { return sbuf[r]; }, fsc);
         }
         __syncthreads();
     }
 }
 
-__global__ void commit_kernel(RoundBuffers rb, JobCounters jc, ApplyArgs a) {
+__global__ void commit_kernel(const ApplyState *st) {
+    const RoundBuffers rb = st->rb;
+    const JobCounters jc = st->jc;
+    const ApplyArgs a = st->a;
     unsigned long long vis = 0, cnt = 0, vd = 0, paths = 0, ball = 0, pred = 0;
     for (uint32_t s = a.lo + blockIdx.x * blockDim.x + threadIdx.x; s < a.hi;
          s += gridDim.x * blockDim.x) {
@@ -320,7 +365,8 @@ __global__ void commit_kernel(RoundBuffers rb, JobCounters jc, ApplyArgs a) {
     }
 }
 
-__global__ void reset_touched_kernel(RoundBuffers rb) {
+__global__ void reset_touched_kernel(const ApplyState *st) {
+    const RoundBuffers rb = st->rb;
     const uint32_t T = *rb.n_touched;
     for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < T; t += gridDim.x * blockDim.x)
         rb.node_cnt[rb.touched[t]] = 0;
@@ -415,25 +461,23 @@ __global__ void peel_map_kernel(JobCounters jc, uint32_t n, const int32_t *lut, 
 
 }  // namespace
 
-cudaError_t apply_round(const RoundBuffers &rb, const JobCounters &jc, const ApplyArgs &a,
-                        cudaStream_t stream) {
-    static bool attr_done = false;
-    if (!attr_done) {
-        cudaFuncSetAttribute(apply_large_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)(kLargeBucket * sizeof(unsigned long long)));
-        attr_done = true;
-    }
-    cudaMemsetAsync(rb.n_touched, 0, sizeof(uint32_t), stream);
-    if (a.pass == 2) signs_kernel<<<64, 256, 0, stream>>>(rb, a);
-    bucket_count_kernel<<<592, 256, 0, stream>>>(rb, a);
-    scan_reduce_kernel<<<kScanBlocks, kScanThreads, 0, stream>>>(rb);
-    scan_top_kernel<<<1, 32, 0, stream>>>(rb, kScanBlocks);
-    scan_down_kernel<<<kScanBlocks, kScanThreads, 0, stream>>>(rb);
-    bucket_scatter_kernel<<<592, 256, 0, stream>>>(rb, a);
-    apply_small_kernel<<<592, kApplyThreads, 0, stream>>>(rb, jc, a);
-    apply_large_kernel<<<148, 1024, kLargeBucket * sizeof(unsigned long long), stream>>>(rb, jc, a);
-    commit_kernel<<<16, 256, 0, stream>>>(rb, jc, a);
-    reset_touched_kernel<<<148, 256, 0, stream>>>(rb);
+cudaError_t apply_init() {
+    return cudaFuncSetAttribute(apply_large_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)(kLargeBucket * sizeof(unsigned long long)));
+}
+
+cudaError_t apply_round(const ApplyState *st, uint32_t *n_touched, cudaStream_t stream) {
+    cudaMemsetAsync(n_touched, 0, sizeof(uint32_t), stream);
+    signs_kernel<<<64, 256, 0, stream>>>(st);
+    bucket_count_kernel<<<592, 256, 0, stream>>>(st);
+    scan_reduce_kernel<<<kScanBlocks, kScanThreads, 0, stream>>>(st);
+    scan_top_kernel<<<1, 32, 0, stream>>>(st, kScanBlocks);
+    scan_down_kernel<<<kScanBlocks, kScanThreads, 0, stream>>>(st);
+    bucket_scatter_kernel<<<592, 256, 0, stream>>>(st);
+    apply_small_kernel<<<592, kApplyThreads, 0, stream>>>(st);
+    apply_large_kernel<<<148, 1024, kLargeBucket * sizeof(unsigned long long), stream>>>(st);
+    commit_kernel<<<16, 256, 0, stream>>>(st);
+    reset_touched_kernel<<<148, 256, 0, stream>>>(st);
     return cudaGetLastError();
 }
 

@@ -66,22 +66,33 @@ struct JobCounters {
 
 struct ApplyArgs {
     uint32_t n;
+    uint32_t n_records;      // path-map records of the round
     uint64_t seed;
     uint32_t first_sample;   // global index of round-local sample 0
     uint32_t lo, hi;         // round-local sample range committed by this call
-    int pass;                // 1 or 2 (pass 2 updates mcrade)
-    int track_cross;         // pass 1 of top-k mode
+    int32_t pass;            // 1 or 2 (pass 2 updates mcrade)
+    int32_t track_cross;     // pass 1 of top-k mode
     uint32_t D;
+};
+
+// Device-resident copies of the three structs above, so that the apply
+// pipeline can be captured once in a CUDA graph and replayed every round.
+struct ApplyState {
+    RoundBuffers rb;
+    JobCounters jc;
+    ApplyArgs a;
 };
 
 // Kernels apply_round launches (one fewer in pass 1: no Rademacher signs).
 constexpr int kApplyRoundKernels = 10;
 
-// Commits round-local samples [lo, hi) of `rb` to `jc`.  Launches only; all
-// sizes that depend on the round are read on the device, so the sequence can
-// be captured in a CUDA graph.
-cudaError_t apply_round(const RoundBuffers &rb, const JobCounters &jc, const ApplyArgs &a,
-                        cudaStream_t stream);
+// Commits round-local samples [a.lo, a.hi) of the round buffers to the job
+// counters, all read from `st` on the device.  Launches only, with fixed grid
+// sizes, so the sequence can be captured in a CUDA graph.  n_touched is the
+// RoundBuffers field of the same struct (passed separately for the memset).
+cudaError_t apply_round(const ApplyState *st, uint32_t *n_touched, cudaStream_t stream);
+// One-time function attributes of the apply kernels (call before capturing).
+cudaError_t apply_init();
 
 // Reduction for one stopping-rule evaluation: per partition and trial the
 // maximum of mcrade (initialised to -n_pairs), per partition the maximum of

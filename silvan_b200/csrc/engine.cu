@@ -1,17 +1,12 @@
-// Host engine (see engine.h): device graph upload, slot and round pools, and
-// the estimator driver that restates Probabilistic::run
-// (silvan/src/Probabilistic.cpp:775-1139) in its one-thread semantics on top
-// of device rounds.
+// Host engine (see engine.h).
 #include "engine.h"
 
 #include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <cstring>
-#include <fstream>
 #include <iomanip>
 #include <map>
-#include <mutex>
 #include <sstream>
 
 #include "bounds.h"
@@ -20,10 +15,11 @@ namespace silvan {
 
 namespace {
 thread_local std::string g_err;
-constexpr uint32_t kRoundSamples = 65536;   // samples per sampler launch
-constexpr uint64_t kInitialRecords = 1u << 22;
-constexpr uint32_t kBlock = 11;             // samples per block (Probabilistic.cpp:829,1061)
+constexpr uint32_t kRoundSamples = 65536;  // samples per job per round
+constexpr uint64_t kInitialRecords = 1u << 20;
+constexpr uint32_t kBlock = 11;  // samples per block (Probabilistic.cpp:829,1061)
 constexpr uint32_t kUncertainCap = 1u << 16;
+constexpr uint32_t kArgRing = 64;
 
 template <typename T>
 int dmalloc(T **p, size_t count) {
@@ -42,6 +38,23 @@ void dfree(T *&p) {
     if (p) cudaFree((void *)p);
     p = nullptr;
 }
+template <typename T>
+int hmalloc(T **p, size_t count) {
+    cudaError_t e = cudaMallocHost((void **)p, sizeof(T) * std::max<size_t>(count, 1));
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        cudaGetLastError();
+        set_error("pinned host allocation failed");
+        return SILVAN_E_OOM;
+    }
+    std::memset((void *)*p, 0, sizeof(T) * std::max<size_t>(count, 1));
+    return SILVAN_OK;
+}
+template <typename T>
+void hfree(T *&p) {
+    if (p) cudaFreeHost((void *)p);
+    p = nullptr;
+}
 }  // namespace
 
 void set_error(const std::string &msg) { g_err = msg; }
@@ -53,14 +66,14 @@ int cuda_status(cudaError_t e, const char *what) {
     return e == cudaErrorMemoryAllocation ? SILVAN_E_OOM : SILVAN_E_CUDA;
 }
 
-#define CK(expr)                                          \
-    do {                                                  \
-        int _rc = cuda_status((expr), #expr);             \
-        if (_rc != SILVAN_OK) return _rc;                 \
+#define CK(expr)                              \
+    do {                                      \
+        int _rc = cuda_status((expr), #expr); \
+        if (_rc != SILVAN_OK) return _rc;     \
     } while (0)
-#define RK(expr)                  \
-    do {                          \
-        int _rc = (expr);         \
+#define RK(expr)                          \
+    do {                                  \
+        int _rc = (expr);                 \
         if (_rc != SILVAN_OK) return _rc; \
     } while (0)
 
@@ -108,6 +121,12 @@ int DeviceGraph::upload() {
     return SILVAN_OK;
 }
 
+uint64_t DeviceGraph::device_bytes() const {
+    uint64_t b = 4ull * (host.n + 1) + 4ull * host.num_edges() + 4ull * host.n;
+    if (host.directed) b += 4ull * (host.n + 1) + 4ull * host.in_adj.size();
+    return b;
+}
+
 DeviceGraph::~DeviceGraph() {
     if (d_in_off != d_out_off) dfree(d_in_off);
     if (d_in_adj != d_out_adj) dfree(d_in_adj);
@@ -118,9 +137,13 @@ DeviceGraph::~DeviceGraph() {
 }
 
 // ---------------------------------------------------------------------------
-// pools
+// SlotPool
 // ---------------------------------------------------------------------------
-int SlotPool::alloc(uint32_t s, uint32_t nn, cudaStream_t st) {
+uint64_t SlotPool::bytes_per_slot(uint64_t n) {
+    return n * (sizeof(NodeRec) + 12) + (uint64_t)kMeetCap * 16;
+}
+
+int SlotPool::alloc(uint32_t s, uint64_t nn, cudaStream_t st) {
     free_all();
     slots = s;
     n = nn;
@@ -132,6 +155,7 @@ int SlotPool::alloc(uint32_t s, uint32_t nn, cudaStream_t st) {
     RK(dmalloc(&meet, (uint64_t)s * kMeetCap));
     RK(dmalloc(&meet_pre, (uint64_t)s * kMeetCap));
     CK(sampler_init_slots(rec, hits, tot, st));
+    CK(cudaStreamSynchronize(st));
     return SILVAN_OK;
 }
 
@@ -142,46 +166,194 @@ void SlotPool::free_all() {
     dfree(touched);
     dfree(meet);
     dfree(meet_pre);
+    slots = 0;
 }
 
-int RoundPool::alloc(uint32_t nn, uint32_t max_samples, uint64_t rec_cap) {
-    free_all();
-    n = nn;
-    RoundBuffers &r = rb;
-    r.max_samples = max_samples;
-    RK(dmalloc(&r.pl, max_samples));
-    RK(dmalloc(&r.np, max_samples));
-    RK(dmalloc(&r.vis, max_samples));
-    RK(dmalloc(&r.status, max_samples));
-    RK(dmalloc(&r.signs, max_samples));
-    RK(dmalloc(&r.ball, max_samples));
-    RK(dmalloc(&r.pred, max_samples));
-    RK(dmalloc(&r.rec_cursor, 1));
-    RK(dmalloc(&r.node_cnt, nn));
-    RK(dmalloc(&r.n_touched, 1));
-    RK(dmalloc(&r.block_sums, 1024));
-    RK(dmalloc(&r.work_counter, 1));
-    CK(cudaMemset(r.node_cnt, 0, sizeof(uint32_t) * nn));
-    return grow_records(rec_cap);
+// ---------------------------------------------------------------------------
+// Engine
+// ---------------------------------------------------------------------------
+Engine::~Engine() {
+    if (stream_) cudaStreamSynchronize(stream_);
+    if (sample_graph_) cudaGraphExecDestroy(sample_graph_);
+    dfree(d_hdr_);
+    dfree(d_segs_);
+    dfree(d_cursors_);
+    hfree(h_hdr_);
+    hfree(h_segs_);
+    hfree(h_cursors_);
+    for (auto &e : ev_)
+        if (e) cudaEventDestroy(e);
+    slots_.free_all();
+    if (stream_) cudaStreamDestroy(stream_);
 }
 
-int RoundPool::grow_records(uint64_t cap) {
-    RoundBuffers &r = rb;
-    dfree(r.recs);
-    dfree(r.touched);
-    dfree(r.bucket_off);
-    dfree(r.entries);
-    r.rec_cap = cap;
-    const uint64_t tcap = std::min<uint64_t>(cap, n) + 1;
-    RK(dmalloc(&r.recs, cap));
-    RK(dmalloc(&r.touched, tcap));
-    RK(dmalloc(&r.bucket_off, tcap + 1));
-    RK(dmalloc(&r.entries, cap));
+int Engine::init(uint64_t n_max, uint32_t slots, uint64_t mem_budget) {
+    CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    for (auto &e : ev_) CK(cudaEventCreate(&e));
+    if (slots == 0) {
+        int dev = 0, sms = 0;
+        CK(cudaGetDevice(&dev));
+        CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        slots = (uint32_t)(sms * std::max(1, sampler_max_ctas_per_sm()));
+    }
+    if (mem_budget == 0) {
+        size_t fr = 0, tot = 0;
+        CK(cudaMemGetInfo(&fr, &tot));
+        mem_budget = fr / 2;
+    }
+    const uint64_t fit = mem_budget / std::max<uint64_t>(SlotPool::bytes_per_slot(n_max), 1);
+    if (fit < slots) slots = (uint32_t)std::max<uint64_t>(fit, 1);
+    RK(slots_.alloc(slots, n_max, stream_));
+    RK(dmalloc(&d_hdr_, 1));
+    RK(hmalloc(&h_hdr_, 1));
+    return ensure_segs(64);
+}
+
+int Engine::ensure_segs(uint32_t nsegs) {
+    if (nsegs <= max_segs_) return SILVAN_OK;
+    uint32_t cap = std::max<uint32_t>(64, max_segs_);
+    while (cap < nsegs) cap *= 2;
+    dfree(d_segs_);
+    dfree(d_cursors_);
+    hfree(h_segs_);
+    hfree(h_cursors_);
+    RK(dmalloc(&d_segs_, cap));
+    RK(dmalloc(&d_cursors_, cap));
+    RK(hmalloc(&h_segs_, cap));
+    RK(hmalloc(&h_cursors_, cap));
+    max_segs_ = cap;
+    if (sample_graph_) cudaGraphExecDestroy(sample_graph_);
+    sample_graph_ = nullptr;
     return SILVAN_OK;
 }
 
-void RoundPool::free_all() {
-    RoundBuffers &r = rb;
+int Engine::round(const std::vector<Job *> &jobs, const std::vector<JobRequest> &reqs,
+                  bool commit, std::vector<uint64_t> *records) {
+    std::vector<uint32_t> idx;
+    for (uint32_t i = 0; i < jobs.size(); i++)
+        if (reqs[i].count > 0) idx.push_back(i);
+    if (records) records->assign(jobs.size(), 0);
+    if (idx.empty()) return SILVAN_OK;
+    RK(ensure_segs((uint32_t)idx.size()));
+    auto fill = [&](uint32_t s, uint32_t j, uint32_t base) {
+        Job *job = jobs[j];
+        const JobRequest &r = reqs[j];
+        const DeviceGraph &G = *job->graph();
+        RoundBuffers &rb = job->round_buffers();
+        SegDesc &S = h_segs_[s];
+        S.out_off = G.d_out_off;
+        S.out_adj = G.d_out_adj;
+        S.in_off = G.d_in_off;
+        S.in_adj = G.d_in_adj;
+        S.cc = G.d_cc;
+        S.n = G.host.n;
+        S.directed = G.host.directed ? 1 : 0;
+        S.seed = job->params().seed;
+        S.alpha = job->alpha();
+        S.np_cap = job->params().np_cap;
+        S.first_sample = r.first_global;
+        S.count = r.count;
+        S.base = base;
+        S.out_pl = rb.pl;
+        S.out_np = rb.np;
+        S.out_vis = rb.vis;
+        S.out_status = rb.status;
+        S.out_ball = rb.ball;
+        S.out_pred = rb.pred;
+        S.recs = rb.recs;
+        S.rec_cursor = d_cursors_ + s;
+        S.rec_cap = rb.rec_cap;
+    };
+    uint32_t total = 0;
+    for (uint32_t s = 0; s < idx.size(); s++) {
+        const JobRequest &r = reqs[idx[s]];
+        if (r.count > kRoundSamples || jobs[idx[s]]->graph()->host.n > slots_.n) {
+            set_error("request larger than the round buffers or graph larger than the slots");
+            return SILVAN_E_BADARG;
+        }
+        fill(s, idx[s], total);
+        total += r.count;
+    }
+    h_hdr_->nsegs = (uint32_t)idx.size();
+    h_hdr_->total = total;
+    h_hdr_->work = 0;
+    const uint32_t grid = std::min<uint32_t>(slots_.slots, total);
+    for (;;) {
+        CK(cudaMemcpyAsync(d_segs_, h_segs_, sizeof(SegDesc) * idx.size(),
+                           cudaMemcpyHostToDevice, stream_));
+        CK(cudaMemcpyAsync(d_hdr_, h_hdr_, sizeof(RoundHeader), cudaMemcpyHostToDevice, stream_));
+        if (!sample_graph_ || graph_grid_ != grid) {
+            if (sample_graph_) cudaGraphExecDestroy(sample_graph_);
+            sample_graph_ = nullptr;
+            SamplerLaunch L{};
+            L.slots = SlotArrays{slots_.rec,  slots_.queue, slots_.hits,    slots_.touched,
+                                 slots_.meet, slots_.meet_pre, slots_.n};
+            L.hdr = d_hdr_;
+            L.segs = d_segs_;
+            cudaGraph_t g = nullptr;
+            CK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+            cudaError_t e1 = sampler_round_begin(L, max_segs_, stream_);
+            cudaError_t e2 = sampler_launch(L, grid, stream_);
+            cudaError_t e3 = cudaStreamEndCapture(stream_, &g);
+            CK(e1);
+            CK(e2);
+            CK(e3);
+            cudaError_t e4 = cudaGraphInstantiate(&sample_graph_, g, 0);
+            cudaGraphDestroy(g);
+            CK(e4);
+            graph_grid_ = grid;
+        }
+        CK(cudaEventRecord(ev_[0], stream_));
+        CK(cudaGraphLaunch(sample_graph_, stream_));
+        CK(cudaEventRecord(ev_[1], stream_));
+        launches_ += 2;
+        CK(cudaMemcpyAsync(h_cursors_, d_cursors_, sizeof(unsigned long long) * idx.size(),
+                           cudaMemcpyDeviceToHost, stream_));
+        CK(cudaStreamSynchronize(stream_));
+        float ms = 0;
+        cudaEventElapsedTime(&ms, ev_[0], ev_[1]);
+        sample_ms_ += ms;
+        bool redo = false;
+        uint32_t base = 0;
+        for (uint32_t s = 0; s < idx.size(); s++) {
+            Job *job = jobs[idx[s]];
+            if (h_cursors_[s] > job->round_buffers().rec_cap) {
+                uint64_t cap = job->round_buffers().rec_cap;
+                while (cap < h_cursors_[s]) cap *= 2;
+                RK(job->grow_records(cap));
+                redo = true;
+            }
+            fill(s, idx[s], base);
+            base += reqs[idx[s]].count;
+        }
+        if (!redo) break;
+        // the path maps did not fit: redraw the round (deterministic)
+        h_hdr_->work = 0;
+    }
+    if (records)
+        for (uint32_t s = 0; s < idx.size(); s++) (*records)[idx[s]] = h_cursors_[s];
+    if (!commit) return SILVAN_OK;
+    CK(cudaEventRecord(ev_[2], stream_));
+    for (uint32_t s = 0; s < idx.size(); s++)
+        RK(jobs[idx[s]]->apply(reqs[idx[s]], (uint32_t)h_cursors_[s], stream_));
+    CK(cudaEventRecord(ev_[3], stream_));
+    CK(cudaEventSynchronize(ev_[3]));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ev_[2], ev_[3]);
+    apply_ms_ += ms;
+    return SILVAN_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Job: allocation and commit
+// ---------------------------------------------------------------------------
+Job::~Job() {
+    if (stream_) cudaStreamSynchronize(stream_);
+    if (apply_graph_) cudaGraphExecDestroy(apply_graph_);
+    delete own_engine_;
+    own_engine_ = nullptr;
+    stream_ = nullptr;
+    RoundBuffers &r = rb_;
     dfree(r.pl);
     dfree(r.np);
     dfree(r.vis);
@@ -190,21 +362,12 @@ void RoundPool::free_all() {
     dfree(r.ball);
     dfree(r.pred);
     dfree(r.recs);
-    dfree(r.rec_cursor);
     dfree(r.node_cnt);
     dfree(r.touched);
     dfree(r.n_touched);
     dfree(r.bucket_off);
     dfree(r.entries);
     dfree(r.block_sums);
-    dfree(r.work_counter);
-}
-
-// ---------------------------------------------------------------------------
-// Job
-// ---------------------------------------------------------------------------
-Job::~Job() {
-    if (stream_) cudaStreamSynchronize(stream_);
     dfree(jc_.approx);
     dfree(jc_.wimpy);
     dfree(jc_.mcrade);
@@ -215,49 +378,72 @@ Job::~Job() {
     dfree(jc_.sc);
     dfree(jc_.partition);
     dfree(jc_.peel_idx);
+    dfree(d_state_);
     dfree(d_red_);
     dfree(d_unc_);
     dfree(d_nunc_);
     dfree(d_lut_);
     dfree(d_hist_);
-    if (h_red_) cudaFreeHost(h_red_);
-    if (h_sc_) cudaFreeHost(h_sc_);
-    if (h_cursor_) cudaFreeHost(h_cursor_);
-    for (auto &e : ev_)
-        if (e) cudaEventDestroy(e);
+    hfree(h_state_);
+    hfree(h_red_);
+    hfree(h_sc_);
     for (auto &e : ev_run_)
         if (e) cudaEventDestroy(e);
-    slots_.free_all();
-    round_.free_all();
-    if (stream_) cudaStreamDestroy(stream_);
+}
+
+int Job::alloc_round(uint32_t max_samples, uint64_t rec_cap) {
+    RoundBuffers &r = rb_;
+    r.max_samples = max_samples;
+    RK(dmalloc(&r.pl, max_samples));
+    RK(dmalloc(&r.np, max_samples));
+    RK(dmalloc(&r.vis, max_samples));
+    RK(dmalloc(&r.status, max_samples));
+    RK(dmalloc(&r.signs, max_samples));
+    RK(dmalloc(&r.ball, max_samples));
+    RK(dmalloc(&r.pred, max_samples));
+    RK(dmalloc(&r.node_cnt, n_));
+    RK(dmalloc(&r.n_touched, 1));
+    RK(dmalloc(&r.block_sums, 1024));
+    r.rec_cursor = nullptr;
+    r.work_counter = nullptr;
+    CK(cudaMemset(r.node_cnt, 0, sizeof(uint32_t) * n_));
+    return grow_records(rec_cap);
+}
+
+int Job::grow_records(uint64_t cap) {
+    RoundBuffers &r = rb_;
+    if (stream_) cudaStreamSynchronize(stream_);
+    dfree(r.recs);
+    dfree(r.touched);
+    dfree(r.bucket_off);
+    dfree(r.entries);
+    r.rec_cap = cap;
+    const uint64_t tcap = std::min<uint64_t>(cap, n_) + 1;
+    RK(dmalloc(&r.recs, cap));
+    RK(dmalloc(&r.touched, tcap));
+    RK(dmalloc(&r.bucket_off, tcap + 1));
+    RK(dmalloc(&r.entries, cap));
+    return SILVAN_OK;
+}
+
+uint64_t Job::device_bytes() const {
+    const uint64_t n = n_;
+    uint64_t b = n * (8 + 8 + 8 * kTrials + 4 + 1 + 4 + 4 + 4 + 4);
+    b += (uint64_t)kRoundSamples * 36 + rb_.rec_cap * (12 + 8) +
+         std::min<uint64_t>(rb_.rec_cap, n) * 8;
+    return b;
 }
 
 int Job::init() {
-    const uint32_t n = g_->host.n;
+    n_ = g_->host.n;
     if (!(p_.eps > 0 && p_.eps < 1) || !(p_.delta > 0 && p_.delta < 1)) {
         set_error("eps and delta must lie in (0, 1)");
         return SILVAN_E_BADARG;
     }
     if (p_.np_cap == 0) p_.np_cap = 1u << 24;
-    CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
-    for (auto &e : ev_) CK(cudaEventCreate(&e));
     for (auto &e : ev_run_) CK(cudaEventCreate(&e));
-    uint32_t slots = p_.slots;
-    if (slots == 0) {
-        int dev = 0, sms = 0;
-        CK(cudaGetDevice(&dev));
-        CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-        int per = std::max(1, sampler_max_ctas_per_sm());
-        slots = (uint32_t)(sms * per);
-        // keep the slot state within half of the free memory
-        size_t fr = 0, tot = 0;
-        CK(cudaMemGetInfo(&fr, &tot));
-        const uint64_t per_slot = (uint64_t)n * (sizeof(NodeRec) + 12) + (uint64_t)kMeetCap * 16;
-        const uint64_t fit = (fr / 2) / std::max<uint64_t>(per_slot, 1);
-        if (fit < slots) slots = (uint32_t)std::max<uint64_t>(fit, 1);
-    }
-    RK(slots_.alloc(slots, n, stream_));
-    RK(round_.alloc(n, kRoundSamples, kInitialRecords));
+    RK(alloc_round(kRoundSamples, kInitialRecords));
+    const uint32_t n = n_;
     RK(dmalloc(&jc_.approx, n));
     RK(dmalloc(&jc_.wimpy, n));
     RK(dmalloc(&jc_.mcrade, (uint64_t)n * kTrials));
@@ -268,129 +454,69 @@ int Job::init() {
     RK(dmalloc(&jc_.sc, 1));
     RK(dmalloc(&jc_.partition, n));
     RK(dmalloc(&jc_.peel_idx, n));
+    RK(dmalloc(&d_state_, 1));
     RK(dmalloc(&d_red_, 1));
     RK(dmalloc(&d_unc_, kUncertainCap));
     RK(dmalloc(&d_nunc_, 1));
-    CK(cudaMallocHost((void **)&h_red_, sizeof(StopReduction)));
-    CK(cudaMallocHost((void **)&h_sc_, sizeof(JobScalars)));
-    CK(cudaMallocHost((void **)&h_cursor_, sizeof(unsigned long long)));
-    CK(cudaMemsetAsync(jc_.approx, 0, sizeof(double) * n, stream_));
-    CK(cudaMemsetAsync(jc_.wimpy, 0, sizeof(double) * n, stream_));
-    CK(cudaMemsetAsync(jc_.mcrade, 0, sizeof(long long) * (uint64_t)n * kTrials, stream_));
-    CK(cudaMemsetAsync(jc_.last_upd, 0, sizeof(uint32_t) * n, stream_));
-    CK(cudaMemsetAsync(jc_.cross_flag, 0, n, stream_));
-    CK(cudaMemsetAsync(jc_.sp_lengths, 0, sizeof(uint64_t) * (g_->diameter + 1), stream_));
-    CK(cudaMemsetAsync(jc_.sc, 0, sizeof(JobScalars), stream_));
-    CK(cudaMemsetAsync(jc_.partition, 0, sizeof(int32_t) * n, stream_));
-    CK(cudaStreamSynchronize(stream_));
+    RK(hmalloc(&h_state_, kArgRing));
+    RK(hmalloc(&h_red_, 1));
+    RK(hmalloc(&h_sc_, 1));
+    CK(cudaMemset(jc_.approx, 0, sizeof(double) * n));
+    CK(cudaMemset(jc_.wimpy, 0, sizeof(double) * n));
+    CK(cudaMemset(jc_.mcrade, 0, sizeof(long long) * (uint64_t)n * kTrials));
+    CK(cudaMemset(jc_.last_upd, 0, sizeof(uint32_t) * n));
+    CK(cudaMemset(jc_.cross_flag, 0, n));
+    CK(cudaMemset(jc_.sp_lengths, 0, sizeof(uint64_t) * (g_->diameter + 1)));
+    CK(cudaMemset(jc_.sc, 0, sizeof(JobScalars)));
+    CK(cudaMemset(jc_.partition, 0, sizeof(int32_t) * n));
+    CK(apply_init());
+    CK(cudaDeviceSynchronize());
     return SILVAN_OK;
 }
 
-// Draws global samples [first_global, first_global + count) and commits them.
-int Job::run_batch(uint32_t first_global, uint32_t count, int pass, bool track_cross) {
-    const DeviceGraph &G = *g_;
-    RoundBuffers &rb = round_.rb;
-    SamplerArgs A{};
-    A.out_off = G.d_out_off;
-    A.out_adj = G.d_out_adj;
-    A.in_off = G.d_in_off;
-    A.in_adj = G.d_in_adj;
-    A.cc = G.d_cc;
-    A.n = G.host.n;
-    A.directed = G.host.directed ? 1 : 0;
-    A.rec = slots_.rec;
-    A.queue = slots_.queue;
-    A.hits = slots_.hits;
-    A.touched = slots_.touched;
-    A.meet = slots_.meet;
-    A.meet_pre = slots_.meet_pre;
-    A.seed = p_.seed;
-    A.alpha = alpha_;
-    A.np_cap = p_.np_cap;
-    A.work_counter = rb.work_counter;
-    A.out_pl = rb.pl;
-    A.out_np = rb.np;
-    A.out_vis = rb.vis;
-    A.out_status = rb.status;
-    A.out_ball = rb.ball;
-    A.out_pred = rb.pred;
-    const bool plain = p_.form == SILVAN_FORM_PLAIN;
-    for (uint32_t done = 0; done < count;) {
-        const uint32_t c = std::min<uint32_t>(count - done, kRoundSamples);
-        A.first_sample = first_global + done;
-        A.count = c;
-        for (;;) {
-            A.recs = rb.recs;
-            A.rec_cursor = rb.rec_cursor;
-            A.rec_cap = rb.rec_cap;
-            CK(cudaMemsetAsync(rb.work_counter, 0, sizeof(uint32_t), stream_));
-            CK(cudaMemsetAsync(rb.rec_cursor, 0, sizeof(unsigned long long), stream_));
-            const uint32_t grid = std::min<uint32_t>(slots_.slots, c);
-            if (!plain) CK(cudaEventRecord(ev_[0], stream_));
-            CK(sampler_launch(A, grid, stream_));
-            launches_ += 1;
-            if (plain) break;
-            CK(cudaEventRecord(ev_[1], stream_));
-            CK(cudaMemcpyAsync(h_cursor_, rb.rec_cursor, sizeof(unsigned long long),
-                               cudaMemcpyDeviceToHost, stream_));
-            CK(cudaStreamSynchronize(stream_));
-            float ms = 0;
-            cudaEventElapsedTime(&ms, ev_[0], ev_[1]);
-            t_sample_ms_ += ms;
-            if (*h_cursor_ <= rb.rec_cap) break;
-            // the round's path maps did not fit: grow and redraw (deterministic)
-            uint64_t cap = rb.rec_cap;
-            while (cap < *h_cursor_) cap *= 2;
-            RK(round_.grow_records(cap));
-        }
-        ApplyArgs ap{};
-        ap.n = G.host.n;
-        ap.seed = p_.seed;
-        ap.first_sample = A.first_sample;
-        ap.pass = pass;
-        ap.track_cross = track_cross ? 1 : 0;
-        ap.D = G.diameter;
-        if (!plain) CK(cudaEventRecord(ev_[2], stream_));
-        for (uint32_t lo = 0; lo < c; lo += kLargeBucket) {
-            ap.lo = lo;
-            ap.hi = std::min<uint32_t>(c, lo + kLargeBucket);
-            CK(apply_round(rb, jc_, ap, stream_));
-            launches_ += kApplyRoundKernels - (pass == 2 ? 0 : 1);
-        }
-        if (!plain) {
-            CK(cudaEventRecord(ev_[3], stream_));
-            CK(cudaEventSynchronize(ev_[3]));
-            float ms = 0;
-            cudaEventElapsedTime(&ms, ev_[2], ev_[3]);
-            t_apply_ms_ += ms;
-        }
-        done += c;
+int Job::capture_apply(cudaStream_t stream) {
+    if (apply_graph_) return SILVAN_OK;
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+    cudaError_t e1 = apply_round(d_state_, rb_.n_touched, stream);
+    cudaError_t e2 = cudaStreamEndCapture(stream, &g);
+    CK(e1);
+    CK(e2);
+    cudaError_t e3 = cudaGraphInstantiate(&apply_graph_, g, 0);
+    cudaGraphDestroy(g);
+    CK(e3);
+    return SILVAN_OK;
+}
+
+// Commits samples [r.first_global, +r.count) whose raw outputs the engine left
+// in rb_, in apply sub-rounds of at most kLargeBucket samples.
+int Job::apply(const JobRequest &r, uint32_t n_records, cudaStream_t stream) {
+    RK(capture_apply(stream));
+    for (uint32_t lo = 0; lo < r.count; lo += kLargeBucket) {
+        ApplyState &st = h_state_[arg_slot_];
+        arg_slot_ = (arg_slot_ + 1) % kArgRing;
+        st.rb = rb_;
+        st.jc = jc_;
+        ApplyArgs &a = st.a;
+        a.n = n_;
+        a.n_records = n_records;
+        a.seed = p_.seed;
+        a.first_sample = r.first_global;
+        a.lo = lo;
+        a.hi = std::min<uint32_t>(r.count, lo + kLargeBucket);
+        a.pass = r.pass;
+        a.track_cross = r.track_cross ? 1 : 0;
+        a.D = g_->diameter;
+        CK(cudaMemcpyAsync(d_state_, &st, sizeof(ApplyState), cudaMemcpyHostToDevice, stream));
+        CK(cudaGraphLaunch(apply_graph_, stream));
+        launches += kApplyRoundKernels;
     }
     return SILVAN_OK;
 }
 
-// Commits samples of the current pass until pass_samples_ == target.
-int Job::sample_range(uint64_t lo, uint64_t hi, int pass, bool track_cross) {
-    (void)lo;
-    if (hi <= pass_samples_) return SILVAN_OK;
-    const uint64_t cnt = hi - pass_samples_;
-    if (global_next_ + cnt >= 0xffffffffull) {
-        set_error("more than 2^32 samples");
-        return SILVAN_E_BADARG;
-    }
-    if (p_.form == SILVAN_FORM_PLAIN) {
-        for (uint64_t done = 0; done < cnt; done += kBlock) {
-            const uint32_t c = (uint32_t)std::min<uint64_t>(kBlock, cnt - done);
-            RK(run_batch((uint32_t)(global_next_ + done), c, pass, track_cross));
-        }
-    } else {
-        RK(run_batch((uint32_t)global_next_, (uint32_t)cnt, pass, track_cross));
-    }
-    global_next_ += cnt;
-    pass_samples_ = hi;
-    return SILVAN_OK;
-}
-
+// ---------------------------------------------------------------------------
+// Job: device reads
+// ---------------------------------------------------------------------------
 int Job::sync_scalars(JobScalars &sc) {
     CK(cudaMemcpyAsync(h_sc_, jc_.sc, sizeof(JobScalars), cudaMemcpyDeviceToHost, stream_));
     CK(cudaStreamSynchronize(stream_));
@@ -402,7 +528,7 @@ int Job::sync_scalars(JobScalars &sc) {
                            : sc.error == SILVAN_E_NP_CAP
                                ? "a sample asked for more shortest paths than the job's cap"
                            : sc.error == SILVAN_E_CAPACITY ? "a per-sample buffer overflowed"
-                                                           : "device sampler error";
+                                                           : "device sampler inconsistency";
         set_error(what);
         return sc.error;
     }
@@ -417,9 +543,17 @@ int Job::read_sp_lengths(std::vector<uint64_t> &out) {
     return SILVAN_OK;
 }
 
+void Job::flush() {
+    if (sink_ && !out_.empty()) {
+        fwrite(out_.data(), 1, out_.size(), sink_);
+        fflush(sink_);
+    }
+    out_.clear();
+}
+
 // Empirical peeling (silvan/src/Probabilistic.cpp:853-871).
 int Job::peel(double a, bool enabled) {
-    const uint32_t n = g_->host.n;
+    const uint32_t n = n_;
     const double ms = (double)pass_samples_;
     part_ids_.clear();
     part_count_.clear();
@@ -428,10 +562,11 @@ int Job::peel(double a, bool enabled) {
         part_ids_.push_back(0);
         part_count_.push_back(n);
         nparts_ = 1;
+        part_host_.assign(n, 0);
         return SILVAN_OK;
     }
     CK(peel_index(jc_, n, ms, a, d_unc_, d_nunc_, kUncertainCap, stream_));
-    launches_ += 3;
+    launches += 1;
     uint32_t nunc = 0;
     CK(cudaMemcpyAsync(&nunc, d_nunc_, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream_));
     CK(cudaStreamSynchronize(stream_));
@@ -456,8 +591,8 @@ int Job::peel(double a, bool enabled) {
             CK(cudaMemcpy(jc_.peel_idx + v, &idx, sizeof(int32_t), cudaMemcpyHostToDevice));
         }
     }
-    // histogram of the indices: they lie in [1, log(m)/log(a) + 1]
-    const int32_t idx_min = std::min(0, host_idx(ms)) ;
+    // the indices lie in [1, log(m)/log(a) + 1]
+    const int32_t idx_min = std::min(0, host_idx(ms));
     const int32_t idx_max = std::max(host_idx(0.0), host_idx(ms)) + 2;
     const int32_t nbins = idx_max - idx_min + 1;
     if (nbins > (1 << 22)) {
@@ -467,6 +602,7 @@ int Job::peel(double a, bool enabled) {
     dfree(d_hist_);
     RK(dmalloc(&d_hist_, nbins));
     CK(peel_hist(jc_, n, idx_min, nbins, d_hist_, stream_));
+    launches += 1;
     std::vector<uint32_t> hist(nbins);
     CK(cudaMemcpyAsync(hist.data(), d_hist_, sizeof(uint32_t) * nbins, cudaMemcpyDeviceToHost,
                        stream_));
@@ -489,6 +625,11 @@ int Job::peel(double a, bool enabled) {
     RK(dmalloc(&d_lut_, nbins));
     CK(cudaMemcpy(d_lut_, lut.data(), sizeof(int32_t) * nbins, cudaMemcpyHostToDevice));
     CK(peel_map(jc_, n, d_lut_, idx_min, nbins, nullptr, stream_));
+    launches += 1;
+    part_host_.resize(n);
+    CK(cudaMemcpyAsync(part_host_.data(), jc_.partition, sizeof(int32_t) * n,
+                       cudaMemcpyDeviceToHost, stream_));
+    CK(cudaStreamSynchronize(stream_));
     return SILVAN_OK;
 }
 
@@ -496,7 +637,7 @@ int Job::peel(double a, bool enabled) {
 // of largest (approx, last update), never-updated nodes after the updated
 // ones in ascending id.
 int Job::ranking(std::vector<uint32_t> &el, std::vector<double> &val) {
-    const uint32_t n = g_->host.n;
+    const uint32_t n = n_;
     std::vector<double> ap(n);
     std::vector<uint32_t> lu(n);
     CK(cudaMemcpyAsync(ap.data(), jc_.approx, sizeof(double) * n, cudaMemcpyDeviceToHost,
@@ -568,20 +709,16 @@ bool Job::check_topk(std::string &outs) {
     }
     std::vector<uint64_t> sp;
     read_sp_lengths(sp);
-    std::vector<int32_t> part_of(el.size());
-    for (size_t i = 0; i < el.size(); i++)
-        cudaMemcpy(&part_of[i], jc_.partition + el[i], sizeof(int32_t), cudaMemcpyDeviceToHost);
+    const double adu = upper_bound_avg_diameter(sp, (int)g_->diameter, dpb, pass_samples_).ub;
     SmallRanking sub(k_), slb(k_);
     uint32_t ins = 0;
     bool rel = true;
-    const uint32_t n = g_->host.n;
-    for (uint64_t i = 0; i < union_sample_ && rel; i++) {
+    const uint32_t n = n_;
+    for (uint64_t i = 0; i < union_sample_ && i < el.size() && rel; i++) {
         const uint32_t node = el[i];
         const double an = val[i] / ms;
-        const double ec = eps_part_[part_of[i]];
+        const double ec = eps_part_[part_host_[node]];
         double lbb = an - ec, ubb = an + ec;
-        const double adu =
-            upper_bound_avg_diameter(sp, (int)g_->diameter, dpb, pass_samples_).ub;
         const double lbr = relative_bound(an, dpb, adu, ms, false, n);
         const double ubr = relative_bound(an, dpb, adu, ms, true, n);
         lbb = fmax(lbb, lbr);
@@ -615,7 +752,7 @@ bool Job::check_topk(std::string &outs) {
             }
             if (!lc || !uc) {
                 out << "   approx_node " << an << "\n";
-                out << "   node_partition_index " << part_ids_[part_of[i]] << "\n";
+                out << "   node_partition_index " << part_ids_[part_host_[node]] << "\n";
             }
             rel = rel && lc && uc;
         } else {
@@ -629,7 +766,7 @@ bool Job::check_topk(std::string &outs) {
         uint32_t cnt = 0;
         for (uint32_t i = 0; i < ins; i++) {
             const double an = val[i] / ms;
-            const double ec = eps_part_[part_of[i]];
+            const double ec = eps_part_[part_host_[el[i]]];
             if (an + ec > lb_topk) {
                 out << i + 1 << ") (" << el[i] << ") " << an - ec << " " << an << " " << an + ec
                     << " " << "\n";
@@ -643,7 +780,7 @@ bool Job::check_topk(std::string &outs) {
 }
 
 // compute_finished_mcrade (silvan/src/Probabilistic.cpp:251-414).
-int Job::stop_check(bool &stop, std::string &outs) {
+int Job::stop_check(bool &stop) {
     std::ostringstream out;
     checks_++;
     const double ms = (double)pass_samples_;
@@ -654,8 +791,8 @@ int Job::stop_check(bool &stop, std::string &outs) {
     out << "EVALUATING STOPPING CONDITION at iteration " << iteration_ << " (m=" << pass_samples_
         << ", d=" << dpb << ")" << "\n";
     const long long init = -(long long)pass_samples_;
-    CK(stop_reduce(jc_, g_->host.n, nparts_, init, d_red_, stream_));
-    launches_ += 2;
+    CK(stop_reduce(jc_, n_, nparts_, init, d_red_, stream_));
+    launches += 2;
     CK(cudaMemcpyAsync(h_red_, d_red_, sizeof(StopReduction), cudaMemcpyDeviceToHost, stream_));
     JobScalars sc;
     RK(sync_scalars(sc));
@@ -701,7 +838,7 @@ int Job::stop_check(bool &stop, std::string &outs) {
         } else {
             out << "   mcrade eps " << sup << "\n";
         }
-        outs += out.str();
+        out_ += out.str();
         return SILVAN_OK;
     }
     std::string tk;
@@ -714,131 +851,112 @@ int Job::stop_check(bool &stop, std::string &outs) {
     } else {
         out << "MCRADE REL DOES NOT STOP " << "\n";
     }
-    outs += out.str();
+    out_ += out.str();
     return SILVAN_OK;
 }
 
 void Job::reset_pass2_counters() {
-    const uint32_t n = g_->host.n;
+    const uint32_t n = n_;
     cudaMemsetAsync(jc_.approx, 0, sizeof(double) * n, stream_);
     cudaMemsetAsync(jc_.wimpy, 0, sizeof(double) * n, stream_);
     cudaMemsetAsync(jc_.mcrade, 0, sizeof(long long) * (uint64_t)n * kTrials, stream_);
     cudaMemsetAsync(jc_.last_upd, 0, sizeof(uint32_t) * n, stream_);
 }
 
-// Probabilistic::run (silvan/src/Probabilistic.cpp:775-1139).
-int Job::run(silvan_result_t *res, FILE *sink) {
-    std::ostringstream out;
-    auto flush = [&]() {
-        if (sink) {
-            std::string s = out.str();
-            fwrite(s.data(), 1, s.size(), sink);
-            fflush(sink);
-        }
-        out.str("");
-        out.clear();
-    };
-    const uint32_t n = g_->host.n;
+// ---------------------------------------------------------------------------
+// Job: the estimator as a state machine (Probabilistic::run,
+// silvan/src/Probabilistic.cpp:775-1139)
+// ---------------------------------------------------------------------------
+int Job::begin(FILE *sink, cudaStream_t stream) {
+    if (phase_ != kInit) {
+        set_error("a job runs once");
+        return SILVAN_E_STATE;
+    }
+    sink_ = sink;
+    stream_ = stream;
     const uint64_t m = g_->host.num_edges();
     const int D = (int)g_->diameter;
     const double eps = p_.eps, delta = p_.delta;
     absolute_ = p_.k == 0;
+    std::ostringstream out;
     out << "estimated diameter of the graph: " << D << "\n";
     out << "time for estimating diameter " << g_->diameter_seconds << "\n";
     uint32_t tau = (uint32_t)fmax(1. / eps * (log(1. / delta)), 1000.);
     tau = (uint32_t)fmax((double)tau, 2 * D * (log(1. / delta)));
     tau_ = tau;
     out << "Starting first pass. Tentative number of samples: " << tau << "\n";
-    const bool peel_on = p_.a > 1;
-    const double a = peel_on ? p_.a : 100. * tau;
+    peel_on_ = p_.a > 1;
+    peel_a_ = peel_on_ ? p_.a : 100. * tau;
     const uint32_t threads = p_.threads ? p_.threads : 1;
-    union_sample_ = std::min(n, (uint32_t)fmax(2 * sqrt((double)m) / threads, p_.k + 20.));
-    k_ = std::min(p_.k, n);
+    union_sample_ = std::min(n_, (uint32_t)fmax(2 * sqrt((double)m) / threads, p_.k + 20.));
+    k_ = std::min(p_.k, n_);
+    out_ += out.str();
     flush();
     CK(cudaMemsetAsync(jc_.sp_lengths, 0, sizeof(uint64_t) * (D + 1), stream_));
-    launches_ = 0;
-    const double start_time = now_seconds();
+    t_start_ = now_seconds();
     CK(cudaEventRecord(ev_run_[0], stream_));
-
-    // ---- pass 1 (:819-846) --------------------------------------------------
-    pass_ = 1;
+    phase_ = kPass1;
     alpha_ = p_.alpha;
     global_next_ = 0;
     pass_samples_ = 0;
-    if (absolute_) {
-        const uint64_t P1 = (uint64_t)kBlock * ((tau + kBlock - 1) / kBlock);
-        RK(sample_range(0, P1, 1, false));
-    } else {
-        // stop after the first block with n_pairs >= tau and at least 1.5 k
-        // nodes whose approx reached 3 (crossings are recorded per sample)
-        uint64_t target = (uint64_t)kBlock * ((tau + kBlock - 1) / kBlock);
-        uint64_t chunk = target;
-        std::vector<uint32_t> cross;
-        for (;;) {
-            RK(sample_range(0, target, 1, true));
-            JobScalars sc;
-            RK(sync_scalars(sc));
-            cross.resize(sc.n_cross);
-            if (sc.n_cross)
-                CK(cudaMemcpy(cross.data(), jc_.cross_sample, sizeof(uint32_t) * sc.n_cross,
-                              cudaMemcpyDeviceToHost));
-            std::sort(cross.begin(), cross.end());
-            // first block end b*11 >= tau with #crossings before it >= 1.5 k
-            uint64_t stop_at = 0;
-            const double need = 1.5 * p_.k;
-            uint64_t first_b = (tau + kBlock - 1) / kBlock;
-            for (uint64_t b = first_b; b * kBlock <= target; b++) {
-                const uint64_t end = b * kBlock;
-                const uint64_t c =
-                    std::lower_bound(cross.begin(), cross.end(), (uint32_t)end) - cross.begin();
-                if ((double)c >= need) {
-                    stop_at = end;
-                    break;
-                }
-            }
-            if (stop_at == 0) {
-                chunk *= 2;
-                target += chunk;
-                continue;
-            }
-            if (stop_at < target) {
-                // roll back: recompute pass 1 up to stop_at
-                CK(cudaMemsetAsync(jc_.approx, 0, sizeof(double) * n, stream_));
-                CK(cudaMemsetAsync(jc_.wimpy, 0, sizeof(double) * n, stream_));
-                CK(cudaMemsetAsync(jc_.last_upd, 0, sizeof(uint32_t) * n, stream_));
-                CK(cudaMemsetAsync(jc_.cross_flag, 0, n, stream_));
-                CK(cudaMemsetAsync(jc_.sp_lengths, 0, sizeof(uint64_t) * (D + 1), stream_));
-                CK(cudaMemsetAsync(jc_.sc, 0, sizeof(JobScalars), stream_));
-                global_next_ = 0;
-                pass_samples_ = 0;
-                RK(sample_range(0, stop_at, 1, true));
-            }
-            break;
-        }
-    }
-    const uint64_t P1 = pass_samples_;
-    JobScalars sc1;
-    RK(sync_scalars(sc1));
-    double sup_bcest;
-    double sup_wv;
-    std::memcpy(&sup_bcest, &sc1.sup_approx_bits, sizeof(double));
-    std::memcpy(&sup_wv, &sc1.sup_wimpy_bits, sizeof(double));
-    out << "First pass finished after " << P1 << " iteration" << "\n";
+    // pass 1 stops after the first 11-sample block with n_pairs >= tau
+    // (:828-845); top-k mode also needs 1.5 k nodes with approx >= 3
+    target_ = (uint64_t)kBlock * ((tau + kBlock - 1) / kBlock);
+    p1_chunk_ = target_;
+    return SILVAN_OK;
+}
 
-    // ---- empirical peeling (:853-889) ---------------------------------------
-    RK(peel(a, peel_on));
+bool Job::next_request(JobRequest &r) {
+    if (phase_ == kDone || phase_ == kInit || error_) return false;
+    uint64_t cnt = target_ - pass_samples_;
+    if (p_.form == SILVAN_FORM_PLAIN) cnt = std::min<uint64_t>(cnt, kBlock);
+    cnt = std::min<uint64_t>(cnt, kRoundSamples);
+    r.first_global = (uint32_t)global_next_;
+    r.count = (uint32_t)cnt;
+    r.pass = phase_ == kPass1 ? 1 : 2;
+    r.track_cross = phase_ == kPass1 && !absolute_;
+    if (global_next_ + cnt >= 0xffffffffull) return false;
+    return cnt > 0;
+}
+
+namespace {
+// The next block end at which pass 2 of the reference acts
+// (Probabilistic.cpp:1060-1087): the omega stop or a schedule check.
+uint64_t pass2_target(uint64_t done, bool m_hat, double omega, uint64_t next_stop,
+                      double last_stop) {
+    uint64_t target = UINT64_MAX;
+    if (m_hat) target = std::min<uint64_t>(target, kBlock * (uint64_t)ceil(omega / kBlock));
+    uint64_t b = (next_stop + kBlock - 1) / kBlock;
+    if (b * kBlock <= done) b = done / kBlock + 1;
+    const uint64_t t = b * kBlock;
+    if ((double)t < last_stop) target = std::min(target, t);
+    if (target == UINT64_MAX || target <= done) target = done + kBlock;
+    return target;
+}
+}  // namespace
+
+int Job::finish_pass1() {
+    const int D = (int)g_->diameter;
+    const double eps = p_.eps, delta = p_.delta;
+    const uint64_t P1 = pass_samples_;
+    p1_samples_ = P1;
+    RK(sync_scalars(sc1_));
+    double sup_bcest, sup_wv;
+    std::memcpy(&sup_bcest, &sc1_.sup_approx_bits, sizeof(double));
+    std::memcpy(&sup_wv, &sc1_.sup_wimpy_bits, sizeof(double));
+    std::ostringstream out;
+    out << "First pass finished after " << P1 << " iteration" << "\n";
+    // empirical peeling (:853-889)
+    RK(peel(peel_a_, peel_on_));
     out << "number_of_non_empty_partitions  " << nparts_ << "\n";
     for (int i = 0; i < nparts_; i++)
         out << "  part. w. index  " << part_ids_[i] << " has " << part_count_[i]
             << " elements, map to " << i << "\n";
-    out << "time for first pass " << now_seconds() - start_time << "\n";
-    out << "void_samples first pass " << sc1.void_samples << "\n";
-    const double t_first = now_seconds() - start_time;
-    flush();
-
-    // ---- bounds and alpha switch (:906-942) ---------------------------------
+    out << "time for first pass " << now_seconds() - t_start_ << "\n";
+    out << "void_samples first pass " << sc1_.void_samples << "\n";
+    t_first_ = now_seconds() - t_start_;
+    // bounds and the alpha switch (:906-942)
     double mns = 0.;
-    alpha_ = p_.alpha;
     if (absolute_) {
         std::vector<uint64_t> sp;
         RK(read_sp_lengths(sp));
@@ -876,8 +994,7 @@ int Job::run(silvan_result_t *res, FILE *sink) {
     CK(cudaMemsetAsync(jc_.sc, 0, sizeof(JobScalars), stream_));
     omega_ = pow(10., 15);
     if (mns > 0.) omega_ = mns;
-
-    // ---- first sample size by bisection (:973-1025) --------------------------
+    // first sample size by bisection (:973-1025)
     uint64_t num_samples = P1;
     double lo = 1. / eps * log(2. / delta), hi = omega_;
     const double svn = sup_wv / (double)P1 + 1 / (double)P1;
@@ -915,50 +1032,93 @@ int Job::run(silvan_result_t *res, FILE *sink) {
     }
     next_stop_ = (uint64_t)first_stop_;
     out << "Starting second phase... " << "\n";
+    out_ += out.str();
     flush();
-
-    // ---- pass 2 (:1054-1102) -------------------------------------------------
-    const double t2_start = now_seconds();
-    pass_ = 2;
+    t2_start_ = now_seconds();
+    phase_ = kPass2;
     pass_samples_ = 0;
-    int reason = 0;
-    for (;;) {
-        // the next block end at which the reference acts
-        uint64_t target = UINT64_MAX;
-        if (p_.m_hat) target = std::min<uint64_t>(target, kBlock * (uint64_t)ceil(omega_ / kBlock));
-        {
-            uint64_t b = (next_stop_ + kBlock - 1) / kBlock;
-            if (b * kBlock <= pass_samples_) b = pass_samples_ / kBlock + 1;
-            const uint64_t t = b * kBlock;
-            if ((double)t < last_stop_) target = std::min(target, t);
-        }
-        if (target == UINT64_MAX) {
-            set_error("stopping schedule has no next evaluation point");
-            return SILVAN_E_STATE;
-        }
-        if (target <= pass_samples_) target = pass_samples_ + kBlock;
-        RK(sample_range(pass_samples_, target, 2, false));
-        if (p_.m_hat && (double)pass_samples_ >= omega_) {
-            reason = 2;
-            break;
-        }
-        if ((double)pass_samples_ < last_stop_ && pass_samples_ >= next_stop_) {
-            bool stop = false;
-            std::string s;
-            RK(stop_check(stop, s));
-            out << s;
-            if (stop) {
-                out << "MCRADE STOPS after seconds " << now_seconds() - start_time << "\n";
-                out << "/* stop_mcrade is true */" << "\n";
-                reason = 1;
-                flush();
-                break;
+    target_ = pass2_target(0, p_.m_hat != 0, omega_, next_stop_, last_stop_);
+    return SILVAN_OK;
+}
+
+int Job::on_committed() {
+    // next_request is a pure function of the state, so the range the engine
+    // just committed is the one it returns now
+    JobRequest last;
+    if (!next_request(last)) return SILVAN_OK;
+    global_next_ += last.count;
+    pass_samples_ += last.count;
+    if (pass_samples_ < target_) return SILVAN_OK;
+    if (phase_ == kPass1) {
+        if (!absolute_ && !p1_final_) {
+            // first block end with n_pairs >= tau and at least 1.5 k nodes
+            // whose approx reached 3
+            JobScalars sc;
+            RK(sync_scalars(sc));
+            std::vector<uint32_t> cross(sc.n_cross);
+            if (sc.n_cross)
+                CK(cudaMemcpy(cross.data(), jc_.cross_sample, sizeof(uint32_t) * sc.n_cross,
+                              cudaMemcpyDeviceToHost));
+            std::sort(cross.begin(), cross.end());
+            uint64_t stop_at = 0;
+            const double need = 1.5 * p_.k;
+            for (uint64_t b = (tau_ + kBlock - 1) / kBlock; b * kBlock <= target_; b++) {
+                const uint64_t c = std::lower_bound(cross.begin(), cross.end(),
+                                                    (uint32_t)(b * kBlock)) -
+                                   cross.begin();
+                if ((double)c >= need) {
+                    stop_at = b * kBlock;
+                    break;
+                }
             }
+            if (stop_at == 0) {
+                p1_chunk_ *= 2;
+                target_ += p1_chunk_;
+                return SILVAN_OK;
+            }
+            p1_final_ = true;
+            if (stop_at < target_) {
+                // redraw pass 1 up to the stopping block (deterministic)
+                const uint32_t n = n_;
+                const int D = (int)g_->diameter;
+                CK(cudaMemsetAsync(jc_.approx, 0, sizeof(double) * n, stream_));
+                CK(cudaMemsetAsync(jc_.wimpy, 0, sizeof(double) * n, stream_));
+                CK(cudaMemsetAsync(jc_.last_upd, 0, sizeof(uint32_t) * n, stream_));
+                CK(cudaMemsetAsync(jc_.cross_flag, 0, n, stream_));
+                CK(cudaMemsetAsync(jc_.sp_lengths, 0, sizeof(uint64_t) * (D + 1), stream_));
+                CK(cudaMemsetAsync(jc_.sc, 0, sizeof(JobScalars), stream_));
+                global_next_ = 0;
+                pass_samples_ = 0;
+                target_ = stop_at;
+                return SILVAN_OK;
+            }
+        }
+        return finish_pass1();
+    }
+    // pass 2 (:1060-1087)
+    bool stop = false;
+    if (p_.m_hat && (double)pass_samples_ >= omega_) {
+        stop = true;
+        stop_reason_ = 2;
+    } else if ((double)pass_samples_ < last_stop_ && pass_samples_ >= next_stop_) {
+        RK(stop_check(stop));
+        if (stop) {
+            std::ostringstream o;
+            o << "MCRADE STOPS after seconds " << now_seconds() - t_start_ << "\n";
+            o << "/* stop_mcrade is true */" << "\n";
+            out_ += o.str();
+            stop_reason_ = 1;
+        } else {
             next_stop_ = (uint64_t)(next_stop_ * 1.2);
             iteration_ += 1;
-            flush();
         }
+        flush();
     }
+    if (!stop) {
+        target_ = pass2_target(pass_samples_, p_.m_hat != 0, omega_, next_stop_, last_stop_);
+        return SILVAN_OK;
+    }
+    // ---- end of the run (:1103-1138) ---------------------------------------
     CK(cudaEventRecord(ev_run_[1], stream_));
     JobScalars sc2;
     RK(sync_scalars(sc2));
@@ -969,24 +1129,27 @@ int Job::run(silvan_result_t *res, FILE *sink) {
     std::memcpy(&sup_b2, &sc2.sup_approx_bits, sizeof(double));
     std::memcpy(&sup_w2, &sc2.sup_wimpy_bits, sizeof(double));
     const uint64_t N2 = pass_samples_;
+    std::ostringstream out;
     out << "out of second pass " << "\n";
-    out << "time for second pass " << t_end - t2_start << "\n";
+    out << "time for second pass " << t_end - t2_start_ << "\n";
     out << "void_samples second pass " << sc2.void_samples << " ("
         << (double)sc2.void_samples / (double)N2 << ")" << "\n";
-    const uint64_t vis_total = sc1.vis_edges + sc2.vis_edges;
+    const uint64_t vis_total = sc1_.vis_edges + sc2.vis_edges;
+    const double t_bfs = own_engine_ ? own_engine_->sample_ms() / 1000.0 : 0.0;
+    const double t_crit = own_engine_ ? own_engine_->apply_ms() / 1000.0 : 0.0;
     if (p_.verbose > 0) {
         if (!absolute_) out << "eps_final_topk " << eps_final_topk_ << "\n";
         out << std::setprecision(6) << "\n" << "Finished after " << N2 << " iterations." << "\n";
         out << "Edges visited: " << vis_total << "\n";
         out << "Average edges visited: " << (N2 ? vis_total / N2 : 0) << "\n";
-        out << "Total time: " << t_end - start_time << "\n";
-        out << "Time bfs: " << t_sample_ms_ / 1000.0 << "\n";
-        out << "Time critical: " << t_apply_ms_ / 1000.0 << "\n";
+        out << "Total time: " << t_end - t_start_ << "\n";
+        out << "Time bfs: " << t_bfs << "\n";
+        out << "Time critical: " << t_crit << "\n";
         out << "Time compute finished: " << 0 << "\n";
         out << "Time mcera: " << 0 << "\n";
         out << "(Printing thread: " << 0 << ")" << "\n";
-        out << "Avg time bfs: " << t_sample_ms_ / 1000.0 << "\n";
-        out << "Avg time critical: " << t_apply_ms_ / 1000.0 << "\n";
+        out << "Avg time bfs: " << t_bfs << "\n";
+        out << "Avg time critical: " << t_crit << "\n";
         out << "Avg time critical (round): " << 0 << "\n";
         out << "Avg time compute finished: " << 0 << "\n";
         out << "Avg time mcera: " << 0 << "\n";
@@ -995,68 +1158,169 @@ int Job::run(silvan_result_t *res, FILE *sink) {
         out << "void_samples: " << sc2.void_samples << "\n";
         out << "num_samples: " << N2 << "\n";
     }
+    out_ += out.str();
     flush();
-    if (!absolute_) {
-        std::vector<uint32_t> el;
-        std::vector<double> val;
-        RK(ranking(el, val));
-        final_rank_el_ = el;
-        final_rank_val_ = val;
+    if (!absolute_) RK(ranking(final_rank_el_, final_rank_val_));
+    silvan_result_t &res = result_;
+    std::memset(&res, 0, sizeof(res));
+    res.first_pass_samples = p1_samples_;
+    res.num_samples = N2;
+    res.vis_edges = vis_total;
+    res.void_samples = sc2.void_samples;
+    res.backtracked_paths = sc2.paths;
+    res.tau = tau_;
+    res.diameter = g_->diameter;
+    res.iteration_index = iteration_;
+    res.num_partitions = nparts_;
+    res.stop_reason = stop_reason_;
+    res.union_sample = union_sample_;
+    res.numresults_topk = numresults_topk_;
+    res.checks = checks_;
+    res.omega = omega_;
+    res.first_stopping_samples = first_stop_;
+    res.last_stopping_samples = last_stop_;
+    res.alpha_sp_sampling = alpha_;
+    res.eps_stop = eps_stop_;
+    res.eps_final_topk = eps_final_topk_;
+    res.sup_bcest = sup_b2 / (double)N2;
+    res.sup_emp_wimpy_var = sup_w2 / (double)N2;
+    res.max_num_samples = max_num_samples_;
+    res.time_total_s = t_end - t_start_;
+    res.time_first_pass_s = t_first_;
+    res.time_sampling_s = t_bfs;
+    res.time_apply_s = t_crit;
+    res.time_device_s = run_ms / 1000.0;
+    res.ball_nodes = sc1_.ball_nodes + sc2.ball_nodes;
+    res.pred_entries = sc1_.pred_entries + sc2.pred_entries;
+    res.kernel_launches = launches + (own_engine_ ? own_engine_->launches() : 0);
+    phase_ = kDone;
+    return SILVAN_OK;
+}
+
+int Job::finish(silvan_result_t *res) {
+    if (phase_ != kDone) {
+        set_error("job has not finished");
+        return SILVAN_E_STATE;
     }
-    finished_ = true;
-    if (res) {
-        std::memset(res, 0, sizeof(*res));
-        res->first_pass_samples = P1;
-        res->num_samples = N2;
-        res->vis_edges = vis_total;
-        res->void_samples = sc2.void_samples;
-        res->backtracked_paths = sc2.paths;
-        res->tau = tau;
-        res->diameter = (uint32_t)D;
-        res->iteration_index = iteration_;
-        res->num_partitions = nparts_;
-        res->stop_reason = reason;
-        res->union_sample = union_sample_;
-        res->numresults_topk = numresults_topk_;
-        res->checks = checks_;
-        res->omega = omega_;
-        res->first_stopping_samples = first_stop_;
-        res->last_stopping_samples = last_stop_;
-        res->alpha_sp_sampling = alpha_;
-        res->eps_stop = eps_stop_;
-        res->eps_final_topk = eps_final_topk_;
-        res->sup_bcest = sup_b2 / (double)N2;
-        res->sup_emp_wimpy_var = sup_w2 / (double)N2;
-        res->max_num_samples = mns;
-        res->time_total_s = t_end - start_time;
-        res->time_first_pass_s = t_first;
-        res->time_sampling_s = t_sample_ms_ / 1000.0;
-        res->time_apply_s = t_apply_ms_ / 1000.0;
-        res->time_device_s = run_ms / 1000.0;
-        res->ball_nodes = sc1.ball_nodes + sc2.ball_nodes;
-        res->pred_entries = sc1.pred_entries + sc2.pred_entries;
-        res->kernel_launches = launches_;
+    if (res) *res = result_;
+    return SILVAN_OK;
+}
+
+int Job::run(silvan_result_t *res, FILE *sink) {
+    if (!own_engine_) {
+        own_engine_ = new Engine();
+        int rc = own_engine_->init(n_, p_.slots, 0);
+        if (rc != SILVAN_OK) return rc;
+    }
+    own_engine_->reset_timers();
+    launches = 0;
+    RK(begin(sink, own_engine_->stream()));
+    std::vector<Job *> jobs{this};
+    std::vector<JobRequest> reqs(1);
+    while (!done()) {
+        if (!next_request(reqs[0])) {
+            set_error("sample index space exhausted");
+            return SILVAN_E_STATE;
+        }
+        int rc = own_engine_->round(jobs, reqs, true, nullptr);
+        if (rc == SILVAN_OK) rc = on_committed();
+        if (rc != SILVAN_OK) {
+            error_ = rc;
+            return rc;
+        }
+    }
+    return finish(res);
+}
+
+int Job::step(uint32_t rounds, silvan_status_t *st, FILE *sink) {
+    if (!own_engine_) {
+        own_engine_ = new Engine();
+        int rc = own_engine_->init(n_, p_.slots, 0);
+        if (rc != SILVAN_OK) return rc;
+    }
+    if (phase_ == kInit) {
+        own_engine_->reset_timers();
+        launches = 0;
+        RK(begin(sink, own_engine_->stream()));
+    }
+    std::vector<Job *> jobs{this};
+    std::vector<JobRequest> reqs(1);
+    for (uint32_t i = 0; i < rounds && !done(); i++) {
+        if (!next_request(reqs[0])) {
+            set_error("sample index space exhausted");
+            return SILVAN_E_STATE;
+        }
+        int rc = own_engine_->round(jobs, reqs, true, nullptr);
+        if (rc == SILVAN_OK) rc = on_committed();
+        if (rc != SILVAN_OK) {
+            error_ = rc;
+            return rc;
+        }
+    }
+    if (st) {
+        JobScalars sc{};
+        if (!done()) RK(sync_scalars(sc));
+        st->samples = done() ? result_.num_samples : pass_samples_;
+        st->void_samples = done() ? result_.void_samples : sc.void_samples;
+        st->vis_edges = done() ? result_.vis_edges : sc.vis_edges;
+        st->backtracked_paths = done() ? result_.backtracked_paths : sc.paths;
+        st->pass = phase_ == kPass1 ? 1 : 2;
+        st->done = done() ? 1 : 0;
     }
     return SILVAN_OK;
 }
 
-int Job::run_to(uint64_t target, silvan_status_t *st) {
-    RK(sample_range(pass_samples_, target, pass_, false));
-    JobScalars sc;
-    int rc = sync_scalars(sc);
-    if (st) {
-        st->samples = pass_samples_;
-        st->void_samples = sc.void_samples;
-        st->vis_edges = sc.vis_edges;
-        st->backtracked_paths = sc.paths;
-        st->pass = pass_;
-        st->error = sc.error;
+int run_batched(const std::vector<Job *> &jobs, uint64_t mem_budget, silvan_result_t *results,
+                FILE *sink) {
+    if (jobs.empty()) return SILVAN_OK;
+    uint64_t n_max = 0;
+    for (Job *j : jobs) {
+        if (j->started()) {
+            set_error("a job runs once");
+            return SILVAN_E_STATE;
+        }
+        n_max = std::max<uint64_t>(n_max, j->nodes());
     }
-    return rc;
+    uint32_t slots = 0;
+    for (Job *j : jobs) slots = std::max(slots, j->params().slots);
+    Engine eng;
+    RK(eng.init(n_max, slots, mem_budget));
+    // the jobs use the engine's stream only while it exists
+    struct Detach {
+        const std::vector<Job *> &js;
+        ~Detach() {
+            for (Job *j : js) j->detach();
+        }
+    } detach{jobs};
+    for (Job *j : jobs) RK(j->begin(sink, eng.stream()));
+    std::vector<Job *> act;
+    std::vector<JobRequest> reqs;
+    for (;;) {
+        act.clear();
+        reqs.clear();
+        for (Job *j : jobs) {
+            if (j->done()) continue;
+            JobRequest r;
+            if (!j->next_request(r)) {
+                set_error("sample index space exhausted");
+                return SILVAN_E_STATE;
+            }
+            act.push_back(j);
+            reqs.push_back(r);
+        }
+        if (act.empty()) break;
+        RK(eng.round(act, reqs, true, nullptr));
+        for (Job *j : act) RK(j->on_committed());
+    }
+    for (size_t i = 0; i < jobs.size(); i++) RK(jobs[i]->finish(&results[i]));
+    return SILVAN_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Job: reads and the replay hook
+// ---------------------------------------------------------------------------
 int Job::read_estimates(double *out, uint32_t n) {
-    if (n != g_->host.n) {
+    if (n != n_) {
         set_error("estimate buffer size does not match the graph");
         return SILVAN_E_BADARG;
     }
@@ -1067,7 +1331,7 @@ int Job::read_estimates(double *out, uint32_t n) {
 }
 
 int Job::read_counters(double *approx, double *wimpy, int64_t *mcrade, int32_t *part) {
-    const uint32_t n = g_->host.n;
+    const uint32_t n = n_;
     if (approx) CK(cudaMemcpy(approx, jc_.approx, sizeof(double) * n, cudaMemcpyDeviceToHost));
     if (wimpy) CK(cudaMemcpy(wimpy, jc_.wimpy, sizeof(double) * n, cudaMemcpyDeviceToHost));
     if (mcrade)
@@ -1083,7 +1347,7 @@ int Job::read_counters(double *approx, double *wimpy, int64_t *mcrade, int32_t *
 }
 
 int Job::read_topk(uint32_t *nodes, double *values, uint32_t cap, uint32_t *count) {
-    if (!finished_ || absolute_) {
+    if (phase_ != kDone || absolute_) {
         set_error("no top-k result");
         return SILVAN_E_STATE;
     }
@@ -1099,76 +1363,42 @@ int Job::read_topk(uint32_t *nodes, double *values, uint32_t cap, uint32_t *coun
 int Job::replay(uint32_t first, uint32_t count, double alpha, std::vector<int32_t> &pl,
                 std::vector<int32_t> &np, std::vector<uint64_t> &vis,
                 std::vector<int32_t> &status, std::vector<PathRec> &recs) {
+    if (!own_engine_) {
+        own_engine_ = new Engine();
+        int rc = own_engine_->init(n_, p_.slots, 0);
+        if (rc != SILVAN_OK) return rc;
+    }
+    stream_ = own_engine_->stream();
     pl.assign(count, 0);
     np.assign(count, 0);
     vis.assign(count, 0);
     status.assign(count, 0);
     recs.clear();
     const double save_alpha = alpha_;
-    const int save_form = p_.form;
     alpha_ = alpha;
-    p_.form = SILVAN_FORM_BATCHED;
-    RoundBuffers &rb = round_.rb;
+    std::vector<Job *> jobs{this};
+    std::vector<JobRequest> reqs(1);
+    std::vector<uint64_t> nrec;
     for (uint32_t done = 0; done < count;) {
         const uint32_t c = std::min<uint32_t>(count - done, kRoundSamples);
-        // sample only: run the sampler part of run_batch without committing
-        SamplerArgs A{};
-        const DeviceGraph &G = *g_;
-        A.out_off = G.d_out_off;
-        A.out_adj = G.d_out_adj;
-        A.in_off = G.d_in_off;
-        A.in_adj = G.d_in_adj;
-        A.cc = G.d_cc;
-        A.n = G.host.n;
-        A.directed = G.host.directed ? 1 : 0;
-        A.rec = slots_.rec;
-        A.queue = slots_.queue;
-        A.hits = slots_.hits;
-        A.touched = slots_.touched;
-        A.meet = slots_.meet;
-        A.meet_pre = slots_.meet_pre;
-        A.seed = p_.seed;
-        A.alpha = alpha_;
-        A.np_cap = p_.np_cap;
-        A.work_counter = rb.work_counter;
-        A.out_pl = rb.pl;
-        A.out_np = rb.np;
-        A.out_vis = rb.vis;
-        A.out_status = rb.status;
-        A.out_ball = rb.ball;
-        A.out_pred = rb.pred;
-        A.first_sample = first + done;
-        A.count = c;
-        for (;;) {
-            A.recs = rb.recs;
-            A.rec_cursor = rb.rec_cursor;
-            A.rec_cap = rb.rec_cap;
-            CK(cudaMemsetAsync(rb.work_counter, 0, sizeof(uint32_t), stream_));
-            CK(cudaMemsetAsync(rb.rec_cursor, 0, sizeof(unsigned long long), stream_));
-            CK(sampler_launch(A, std::min<uint32_t>(slots_.slots, c), stream_));
-            CK(cudaMemcpyAsync(h_cursor_, rb.rec_cursor, sizeof(unsigned long long),
-                               cudaMemcpyDeviceToHost, stream_));
-            CK(cudaStreamSynchronize(stream_));
-            if (*h_cursor_ <= rb.rec_cap) break;
-            uint64_t cap = rb.rec_cap;
-            while (cap < *h_cursor_) cap *= 2;
-            RK(round_.grow_records(cap));
-        }
-        CK(cudaMemcpy(pl.data() + done, rb.pl, sizeof(int32_t) * c, cudaMemcpyDeviceToHost));
-        CK(cudaMemcpy(np.data() + done, rb.np, sizeof(int32_t) * c, cudaMemcpyDeviceToHost));
-        CK(cudaMemcpy(vis.data() + done, rb.vis, sizeof(uint64_t) * c, cudaMemcpyDeviceToHost));
-        CK(cudaMemcpy(status.data() + done, rb.status, sizeof(int32_t) * c,
+        reqs[0].first_global = first + done;
+        reqs[0].count = c;
+        reqs[0].pass = 1;
+        RK(own_engine_->round(jobs, reqs, false, &nrec));
+        CK(cudaMemcpy(pl.data() + done, rb_.pl, sizeof(int32_t) * c, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(np.data() + done, rb_.np, sizeof(int32_t) * c, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(vis.data() + done, rb_.vis, sizeof(uint64_t) * c, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(status.data() + done, rb_.status, sizeof(int32_t) * c,
                       cudaMemcpyDeviceToHost));
         const size_t r0 = recs.size();
-        recs.resize(r0 + *h_cursor_);
-        if (*h_cursor_)
-            CK(cudaMemcpy(recs.data() + r0, rb.recs, sizeof(PathRec) * (*h_cursor_),
+        recs.resize(r0 + nrec[0]);
+        if (nrec[0])
+            CK(cudaMemcpy(recs.data() + r0, rb_.recs, sizeof(PathRec) * nrec[0],
                           cudaMemcpyDeviceToHost));
         for (size_t i = r0; i < recs.size(); i++) recs[i].sample += done;
         done += c;
     }
     alpha_ = save_alpha;
-    p_.form = save_form;
     return SILVAN_OK;
 }
 

@@ -1,4 +1,12 @@
-// Host engine: device graph, job state and the estimator driver.
+// Host engine: device graph, sampler engine and the estimator state machine.
+//
+// An Engine owns sampler slots sized for the largest graph it serves and runs
+// sampler rounds over any number of jobs at once (one persistent launch whose
+// work is the concatenation of every job's request).  A Job owns its counters
+// and round buffers and restates Probabilistic::run
+// (silvan/src/Probabilistic.cpp:775-1139) as a state machine: it asks for the
+// next range of samples, and after the engine has drawn and committed them it
+// evaluates the schedule events the reference evaluates at that point.
 #pragma once
 #include <cstdint>
 #include <cstdio>
@@ -16,6 +24,7 @@ namespace silvan {
 
 void set_error(const std::string &msg);
 int cuda_status(cudaError_t e, const char *what);
+double now_seconds();
 
 struct DeviceGraph {
     HostGraph host;
@@ -30,85 +39,172 @@ struct DeviceGraph {
     int device = 0;
 
     int upload();
+    uint64_t device_bytes() const;
     ~DeviceGraph();
 };
 
-// Per-slot sampler state plus per-round buffers.
+// Per-slot sampler state.
 struct SlotPool {
-    uint32_t slots = 0, n = 0;
+    uint32_t slots = 0;
+    uint64_t n = 0;
     NodeRec *rec = nullptr;
     uint32_t *queue = nullptr, *hits = nullptr, *touched = nullptr;
     uint2 *meet = nullptr;
     uint64_t *meet_pre = nullptr;
-    int alloc(uint32_t slots, uint32_t n, cudaStream_t s);
+    int alloc(uint32_t slots, uint64_t n, cudaStream_t s);
     void free_all();
+    static uint64_t bytes_per_slot(uint64_t n);
     ~SlotPool() { free_all(); }
 };
 
-struct RoundPool {
-    RoundBuffers rb{};
-    uint32_t n = 0;
-    int alloc(uint32_t n, uint32_t max_samples, uint64_t rec_cap);
-    int grow_records(uint64_t rec_cap);
-    void free_all();
-    ~RoundPool() { free_all(); }
+struct JobRequest {
+    uint32_t first_global = 0;  // global sample index of the range's first sample
+    uint32_t count = 0;
+    int pass = 1;
+    bool track_cross = false;
+};
+
+class Job;
+
+class Engine {
+  public:
+    ~Engine();
+    // slots = 0 picks occupancy x SM count, capped by `mem_budget` bytes
+    // (0 = half of the free device memory)
+    int init(uint64_t n_max, uint32_t slots, uint64_t mem_budget);
+    bool ready() const { return slots_.slots > 0; }
+    uint64_t n_max() const { return slots_.n; }
+    uint32_t slots() const { return slots_.slots; }
+    cudaStream_t stream() const { return stream_; }
+    // Draws every job's requested range in one persistent launch, then
+    // commits each range to its job (ordered apply).  Grows a job's record
+    // buffer and redraws the round when the path maps did not fit.
+    // With commit == false the round only draws (replay); `records` receives
+    // the number of path-map records of each job.
+    int round(const std::vector<Job *> &jobs, const std::vector<JobRequest> &reqs,
+              bool commit = true, std::vector<uint64_t> *records = nullptr);
+    uint64_t launches() const { return launches_; }
+    float sample_ms() const { return sample_ms_; }
+    float apply_ms() const { return apply_ms_; }
+    void reset_timers() {
+        sample_ms_ = apply_ms_ = 0;
+        launches_ = 0;
+    }
+
+  private:
+    int ensure_segs(uint32_t nsegs);
+    SlotPool slots_;
+    cudaStream_t stream_ = nullptr;
+    RoundHeader *d_hdr_ = nullptr, *h_hdr_ = nullptr;
+    SegDesc *d_segs_ = nullptr, *h_segs_ = nullptr;
+    unsigned long long *d_cursors_ = nullptr, *h_cursors_ = nullptr;
+    uint32_t max_segs_ = 0;
+    cudaGraphExec_t sample_graph_ = nullptr;
+    uint32_t graph_grid_ = 0;
+    cudaEvent_t ev_[4] = {nullptr, nullptr, nullptr, nullptr};
+    float sample_ms_ = 0, apply_ms_ = 0;
+    uint64_t launches_ = 0;
 };
 
 class Job {
   public:
     Job(DeviceGraph *g, const silvan_params_t &p) : g_(g), p_(p) {}
     ~Job();
-    int init();
+    int init();  // counters and round buffers; no sampler slots
+    uint64_t device_bytes() const;
+
+    // single-job run on an engine of its own (created on first use)
     int run(silvan_result_t *res, FILE *sink);
-    // step-wise: commit samples of the current pass up to `target`
-    int run_to(uint64_t target, silvan_status_t *st);
-    int read_estimates(double *out, uint32_t n);
-    int read_counters(double *approx, double *wimpy, int64_t *mcrade, int32_t *part);
-    int read_topk(uint32_t *nodes, double *values, uint32_t cap, uint32_t *count);
+    // at most `rounds` rounds of the job's schedule on its own engine
+    int step(uint32_t rounds, silvan_status_t *st, FILE *sink);
+
+    // ---- state machine used by Engine::round drivers -------------------------
+    int begin(FILE *sink, cudaStream_t stream);
+    bool done() const { return phase_ == kDone; }
+    bool next_request(JobRequest &r);
+    int on_committed();  // after the last requested range was drawn and committed
+    int finish(silvan_result_t *res);
+    int error() const { return error_; }
+    uint32_t nodes() const { return n_; }
+    // forget the stream of an engine that is going away
+    void detach() {
+        if (stream_) cudaStreamSynchronize(stream_);
+        stream_ = own_engine_ ? own_engine_->stream() : nullptr;
+        sink_ = nullptr;
+    }
+    bool started() const { return phase_ != kInit; }
 
     // per-sample replay (parity hook): raw sampler output of [first, first+count)
     int replay(uint32_t first, uint32_t count, double alpha, std::vector<int32_t> &pl,
                std::vector<int32_t> &np, std::vector<uint64_t> &vis,
                std::vector<int32_t> &status, std::vector<PathRec> &recs);
 
+    int read_estimates(double *out, uint32_t n);
+    int read_counters(double *approx, double *wimpy, int64_t *mcrade, int32_t *part);
+    int read_topk(uint32_t *nodes, double *values, uint32_t cap, uint32_t *count);
+
+    // ---- used by Engine -------------------------------------------------------
+    DeviceGraph *graph() const { return g_; }
+    const silvan_params_t &params() const { return p_; }
+    double alpha() const { return alpha_; }
+    RoundBuffers &round_buffers() { return rb_; }
+    int grow_records(uint64_t cap);
+    // commits the drawn range (records of the round already in rb_)
+    int apply(const JobRequest &r, uint32_t n_records, cudaStream_t stream);
+    uint64_t launches = 0;
+
   private:
-    int sample_range(uint64_t lo, uint64_t hi, int pass, bool track_cross);
-    int run_batch(uint32_t first_global, uint32_t count, int pass, bool track_cross);
+    enum Phase { kInit, kPass1, kPass2, kDone };
+    int alloc_round(uint32_t max_samples, uint64_t rec_cap);
+    int capture_apply(cudaStream_t stream);
     int sync_scalars(JobScalars &sc);
     int read_sp_lengths(std::vector<uint64_t> &out);
     int peel(double a, bool enabled);
-    int stop_check(bool &stop, std::string &out);
+    int finish_pass1();
+    int stop_check(bool &stop);
     int ranking(std::vector<uint32_t> &el, std::vector<double> &val);
     bool check_topk(std::string &out);
     void reset_pass2_counters();
+    void flush();
 
     DeviceGraph *g_;
     silvan_params_t p_;
-    cudaStream_t stream_ = nullptr;
-    SlotPool slots_;
-    RoundPool round_;
+    Engine *own_engine_ = nullptr;
+    cudaStream_t stream_ = nullptr;  // stream of the engine driving the job
+    RoundBuffers rb_{};
+    uint32_t n_ = 0;
     JobCounters jc_{};
+    ApplyState *d_state_ = nullptr;
+    ApplyState *h_state_ = nullptr;  // pinned ring of kArgRing entries
+    uint32_t arg_slot_ = 0;
+    cudaGraphExec_t apply_graph_ = nullptr;
     StopReduction *d_red_ = nullptr;
     StopReduction *h_red_ = nullptr;  // pinned
     JobScalars *h_sc_ = nullptr;      // pinned
-    unsigned long long *h_cursor_ = nullptr;  // pinned
     uint32_t *d_unc_ = nullptr, *d_nunc_ = nullptr;
     int32_t *d_lut_ = nullptr;
     uint32_t *d_hist_ = nullptr;
-    cudaEvent_t ev_[4] = {nullptr, nullptr, nullptr, nullptr};
     cudaEvent_t ev_run_[2] = {nullptr, nullptr};
-    uint64_t launches_ = 0;
+    FILE *sink_ = nullptr;
+    std::string out_;  // pending status lines
 
     // estimator state (members of Probabilistic, silvan/include/Probabilistic.h:59-110)
+    Phase phase_ = kInit;
+    int error_ = 0;
     bool absolute_ = true;
+    bool peel_on_ = true;
+    double peel_a_ = 2.0;
     uint32_t k_ = 0, union_sample_ = 0, tau_ = 0;
-    uint64_t global_next_ = 0;  // global index of the next sample
-    uint64_t pass_samples_ = 0; // samples committed in the current pass
-    int pass_ = 1;
+    uint64_t global_next_ = 0;   // global index of the next sample to draw
+    uint64_t pass_samples_ = 0;  // samples committed in the current pass
+    uint64_t target_ = 0;        // sample count of the next schedule event
+    uint64_t p1_chunk_ = 0;      // top-k pass 1: speculative chunk size
+    bool p1_final_ = false;      // top-k pass 1: the stopping block is known
     double alpha_ = 2.3;
     int nparts_ = 1;
-    std::vector<int> part_ids_;        // raw peeling index of each dense id
+    std::vector<int> part_ids_;  // raw peeling index of each dense id
     std::vector<uint32_t> part_count_;
+    std::vector<int32_t> part_host_;
     std::vector<double> eps_part_;
     double omega_ = 0, first_stop_ = 0, last_stop_ = 0, dfpb_ = 1.0;
     uint64_t next_stop_ = 0;
@@ -118,14 +214,18 @@ class Job {
     double eps_stop_ = -1;
     uint32_t checks_ = 0;
     double max_num_samples_ = 0;
-    double sup_bcest_p1_ = 0, sup_wv_p1_ = 0;
-    uint64_t void_p1_ = 0;
-    float t_sample_ms_ = 0, t_apply_ms_ = 0;
+    uint64_t p1_samples_ = 0;
+    JobScalars sc1_{};
+    int stop_reason_ = 0;
+    double t_start_ = 0, t_first_ = 0, t2_start_ = 0;
     std::vector<uint32_t> final_rank_el_;
     std::vector<double> final_rank_val_;
-    bool finished_ = false;
+    silvan_result_t result_{};
 };
 
-double now_seconds();
+// Runs jobs to completion, one sampler launch per round for all unfinished
+// jobs (multi-graph batching).
+int run_batched(const std::vector<Job *> &jobs, uint64_t mem_budget, silvan_result_t *results,
+                FILE *sink);
 
 }  // namespace silvan

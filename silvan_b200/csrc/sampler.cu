@@ -39,6 +39,7 @@ constexpr int kWarps = kSamplerBlock / 32;
 constexpr int kItems = 4;                      // scan items per lane per tile
 constexpr int kTile = kSamplerBlock * kItems;  // scan items per tile
 constexpr int kChunk = 2048;                   // frontier nodes staged at once
+constexpr int kMaxLevels = 256;                // levels per side with recorded bounds
 
 struct SamplerSmem {
     uint32_t f_node[kChunk];
@@ -64,7 +65,11 @@ struct SamplerSmem {
     int32_t status;
     int32_t nonmono;
     unsigned long long W;
-    uint32_t chunk_total;
+    uint32_t work;
+    // queue segment of every BFS level: side (U = 0, V = 1), depth
+    uint32_t lvl_lo[2][kMaxLevels];
+    uint32_t lvl_hi[2][kMaxLevels];
+    SegDesc seg;  // the segment of the sample in flight
 };
 
 __device__ __forceinline__ uint32_t lanemask_lt() {
@@ -113,25 +118,80 @@ __device__ __forceinline__ void rec_reset(NodeRec *r) {
     p[1] = make_uint4(0xffffffffu, 0xffffffffu, 0u, 0u);  // first = ~0, last = 0
 }
 
-// Predecessor of rank t (queue order) of node a, 0 < t < cnt - 1.
-__device__ uint32_t middle_pred(const SamplerArgs &A, const NodeRec *rec, uint32_t a,
-                                uint32_t st_a, uint32_t t) {
+// Predecessor of rank t (queue order) of node a, 0 < t < cnt - 1.  The
+// predecessors of a node at depth d are the nodes of level d-1 of its side
+// whose row (in the expansion direction) contains it, in queue order.  Two
+// equivalent searches, whichever reads less:
+//   level scan: walk the level's queue segment, binary-search a in each row;
+//   reverse scan: walk a's reverse row, keep the candidates on level d-1 and
+//                 rank them by their own queue position (their first hit).
+__device__ uint32_t middle_pred(const SegDesc &A, const SamplerSmem &s, const NodeRec *rec,
+                                const uint32_t *queue, uint32_t a, uint32_t st_a, uint32_t t,
+                                int32_t &status) {
     const uint32_t side = st_side(st_a);
-    const uint32_t want = st_make(side, st_dist(st_a) - 1u);
-    const uint32_t *off = side == kSideU ? A.in_off : A.out_off;
-    const uint32_t *adj = side == kSideU ? A.in_adj : A.out_adj;
-    const uint32_t b = off[a], e = off[a + 1];
+    const uint32_t dprev = st_dist(st_a) - 1u;
+    const uint32_t want = st_make(side, dprev);
+    const uint32_t *roff = side == kSideU ? A.in_off : A.out_off;
+    const uint32_t *radj = side == kSideU ? A.in_adj : A.out_adj;
+    const uint32_t *foff = side == kSideU ? A.out_off : A.in_off;
+    const uint32_t *fadj = side == kSideU ? A.out_adj : A.in_adj;
+    const uint32_t rb = roff[a], re = roff[a + 1];
+    if (dprev < (uint32_t)kMaxLevels) {
+        const uint32_t lo = s.lvl_lo[side - 1][dprev], hi = s.lvl_hi[side - 1][dprev];
+        if ((uint64_t)(hi - lo) * 24u < (uint64_t)(re - rb)) {
+            uint32_t seen = 0;
+            for (uint32_t i = lo; i < hi; i++) {
+                const uint32_t x = __ldcg(&queue[i]);
+                uint32_t l = foff[x], h = foff[x + 1];
+                while (l < h) {  // first entry >= a
+                    const uint32_t mid = (l + h) >> 1;
+                    if (fadj[mid] < a) l = mid + 1;
+                    else h = mid;
+                }
+                if (l < foff[x + 1] && fadj[l] == a) {
+                    if (seen == t) return x;
+                    seen++;
+                }
+            }
+            status = SILVAN_E_STATE;
+            return a;
+        }
+    }
+    // reverse scan with a bounded buffer of the t+1 smallest keys
+    constexpr uint32_t kBuf = 16;
+    if (t < kBuf) {
+        unsigned long long key[kBuf];
+        uint32_t node[kBuf];
+        uint32_t nb = 0;
+        for (uint32_t k = rb; k < re; k++) {
+            const uint32_t x = radj[k];
+            if (__ldcg(&rec[x].st) != want) continue;
+            const unsigned long long kx = __ldcg(&rec[x].first) >> 32;
+            if (nb == t + 1 && kx >= key[t]) continue;
+            uint32_t p = nb < t + 1 ? nb++ : t;
+            while (p > 0 && key[p - 1] > kx) {
+                key[p] = key[p - 1];
+                node[p] = node[p - 1];
+                p--;
+            }
+            key[p] = kx;
+            node[p] = x;
+        }
+        if (nb == t + 1) return node[t];
+        status = SILVAN_E_STATE;
+        return a;
+    }
     unsigned long long prev = 0;
     bool have_prev = false;
     uint32_t bx = a;
     for (uint32_t r = 0; r <= t; r++) {
         unsigned long long best = ~0ull;
-        for (uint32_t k = b; k < e; k++) {
-            uint32_t x = adj[k];
+        for (uint32_t k = rb; k < re; k++) {
+            const uint32_t x = radj[k];
             if (__ldcg(&rec[x].st) != want) continue;
-            unsigned long long key = __ldcg(&rec[x].first) >> 32;
-            if ((!have_prev || key > prev) && key < best) {
-                best = key;
+            const unsigned long long kx = __ldcg(&rec[x].first) >> 32;
+            if ((!have_prev || kx > prev) && kx < best) {
+                best = kx;
                 bx = x;
             }
         }
@@ -150,7 +210,7 @@ __device__ __forceinline__ void note_hit(uint32_t *hits, uint32_t *touched, Samp
 }
 
 // Expands one BFS level of `side` (silvan/src/Sp_sampler.cpp:89-143).
-__device__ void expand_level(const SamplerArgs &A, SamplerSmem &s, NodeRec *rec,
+__device__ void expand_level(const SegDesc &A, SamplerSmem &s, NodeRec *rec,
                              uint32_t *queue, uint2 *meet, uint32_t side, uint32_t lo,
                              uint32_t hi, uint32_t depth) {
     const uint32_t *off = side == kSideU ? A.out_off : A.in_off;
@@ -316,22 +376,45 @@ __device__ void expand_level(const SamplerArgs &A, SamplerSmem &s, NodeRec *rec,
     __syncthreads();
 }
 
-__global__ void __launch_bounds__(kSamplerBlock, 2) sampler_kernel(SamplerArgs A) {
+__global__ void __launch_bounds__(kSamplerBlock, 2) sampler_kernel(SamplerLaunch L) {
     __shared__ SamplerSmem s;
     const uint32_t slot = blockIdx.x;
-    const uint64_t base = (uint64_t)slot * A.n;
-    NodeRec *rec = A.rec + base;
-    uint32_t *queue = A.queue + base;
-    uint32_t *hits = A.hits + base;
-    uint32_t *touched = A.touched + base;
-    uint2 *meet = A.meet + (uint64_t)slot * kMeetCap;
-    uint64_t *mpre = A.meet_pre + (uint64_t)slot * kMeetCap;
+    const uint64_t base = (uint64_t)slot * L.slots.stride;
+    NodeRec *rec = L.slots.rec + base;
+    uint32_t *queue = L.slots.queue + base;
+    uint32_t *hits = L.slots.hits + base;
+    uint32_t *touched = L.slots.touched + base;
+    uint2 *meet = L.slots.meet + (uint64_t)slot * kMeetCap;
+    uint64_t *mpre = L.slots.meet_pre + (uint64_t)slot * kMeetCap;
+    const uint32_t total = L.hdr->total;
+    const uint32_t nsegs = L.hdr->nsegs;
+    const SegDesc &A = s.seg;
 
     for (;;) {
-        if (threadIdx.x == 0) s.sample = atomicAdd(A.work_counter, 1u);
+        if (threadIdx.x == 0) {
+            const uint32_t w = atomicAdd(&L.hdr->work, 1u);
+            s.work = w;
+            if (w < total) {
+                // segment owning work index w: last segment with base <= w
+                uint32_t l = 0, h = nsegs;
+                while (h - l > 1) {
+                    const uint32_t mid = (l + h) >> 1;
+                    if (L.segs[mid].base <= w) l = mid;
+                    else h = mid;
+                }
+                s.sample = l;
+            }
+        }
         __syncthreads();
-        const uint32_t sl = s.sample;
-        if (sl >= A.count) break;
+        if (s.work >= total) break;
+        {
+            const uint32_t *src = reinterpret_cast<const uint32_t *>(&L.segs[s.sample]);
+            uint32_t *dst = reinterpret_cast<uint32_t *>(&s.seg);
+            for (uint32_t i = threadIdx.x; i < sizeof(SegDesc) / 4; i += kSamplerBlock)
+                dst[i] = src[i];
+        }
+        __syncthreads();
+        const uint32_t sl = s.work - A.base;
         const uint32_t gidx = A.first_sample + sl;
 
         // ---- endpoints (Sp_sampler.cpp:46,58-60) and void test (:62-74) -------
@@ -372,6 +455,10 @@ __global__ void __launch_bounds__(kSamplerBlock, 2) sampler_kernel(SamplerArgs A
             rec[v].sigma = 1;
             queue[0] = u;
             queue[1] = v;
+            s.lvl_lo[0][0] = 0;
+            s.lvl_hi[0][0] = 1;
+            s.lvl_lo[1][0] = 1;
+            s.lvl_hi[1][0] = 2;
             s.end_q = 2;
             s.start_u = 0;
             s.end_u = 1;
@@ -396,6 +483,10 @@ __global__ void __launch_bounds__(kSamplerBlock, 2) sampler_kernel(SamplerArgs A
             __syncthreads();
             expand_level(A, s, rec, queue, meet, exp_side, lo, hi, depth);
             if (threadIdx.x == 0) {
+                if (depth + 1 < (uint32_t)kMaxLevels) {
+                    s.lvl_lo[side_u ? 0 : 1][depth + 1] = q0;
+                    s.lvl_hi[side_u ? 0 : 1][depth + 1] = s.end_q;
+                }
                 if (side_u) {
                     s.start_u = q0;
                     s.end_u = s.end_q;
@@ -522,7 +613,12 @@ __global__ void __launch_bounds__(kSamplerBlock, 2) sampler_kernel(SamplerArgs A
                                 a = (uint32_t)__ldcg(
                                     reinterpret_cast<const unsigned long long *>(&rec[a].last));
                             } else {
-                                a = middle_pred(A, rec, a, sta, t);
+                                int32_t e = 0;
+                                a = middle_pred(A, s, rec, queue, a, sta, t, e);
+                                if (e) {
+                                    s.status = e;
+                                    break;
+                                }
                             }
                         }
                     }
@@ -573,6 +669,12 @@ __global__ void __launch_bounds__(kSamplerBlock, 2) sampler_kernel(SamplerArgs A
     }
 }
 
+__global__ void round_begin_kernel(SamplerLaunch L, uint32_t max_segs) {
+    const uint32_t ns = min(L.hdr->nsegs, max_segs);
+    for (uint32_t i = threadIdx.x; i < ns; i += blockDim.x) *L.segs[i].rec_cursor = 0ull;
+    if (threadIdx.x == 0) L.hdr->work = 0;
+}
+
 __global__ void init_slots_kernel(NodeRec *rec, uint32_t *hits, uint64_t total) {
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < total;
          i += (uint64_t)gridDim.x * blockDim.x) {
@@ -589,9 +691,14 @@ cudaError_t sampler_init_slots(NodeRec *rec, uint32_t *hits, uint64_t total_node
     return cudaGetLastError();
 }
 
-cudaError_t sampler_launch(const SamplerArgs &a, uint32_t grid, cudaStream_t stream) {
+cudaError_t sampler_round_begin(const SamplerLaunch &L, uint32_t max_segs, cudaStream_t stream) {
+    round_begin_kernel<<<1, 256, 0, stream>>>(L, max_segs);
+    return cudaGetLastError();
+}
+
+cudaError_t sampler_launch(const SamplerLaunch &L, uint32_t grid, cudaStream_t stream) {
     if (grid == 0) return cudaSuccess;
-    sampler_kernel<<<grid, kSamplerBlock, 0, stream>>>(a);
+    sampler_kernel<<<grid, kSamplerBlock, 0, stream>>>(L);
     return cudaGetLastError();
 }
 

@@ -18,8 +18,14 @@ def compare(a, b):
             raise AssertionError(f"{f} differs first at {bad[:5]}")
 
 
-@pytest.mark.parametrize("name", sorted(SMALL_GRAPHS))
-@pytest.mark.parametrize("alpha", [2.3, -1.0])
+# Lattices ask for astronomically many paths per sample at alpha > 0 (the
+# reference does not finish on them, silvan/src/Sp_sampler.cpp:166-170), so the
+# grid is replayed in single-path mode only.
+CASES = [(n, a) for n in sorted(SMALL_GRAPHS) for a in (2.3, -1.0)
+         if not (n.startswith("grid") and a > 0)]
+
+
+@pytest.mark.parametrize("name,alpha", CASES)
 def test_replay_matches_oracle(sb, port, small_graphs, name, alpha):
     hg, csr, directed = small_graphs[name]
     g = sb.Graph.from_host(hg)
