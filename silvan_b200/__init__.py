@@ -408,10 +408,11 @@ class Probabilistic:
             self.result = res.as_dict()
         return d
 
-    def get_centrality(self):
-        """approx[v] / num_samples for every node."""
+    def get_centrality(self, out=None):
+        """approx[v] / num_samples for every node (into `out` when given)."""
         n = self.graph.n
-        out = np.zeros(n, np.float64)
+        if out is None:
+            out = np.zeros(n, np.float64)
         _check(load().silvan_read_estimates(self.h, _p(out), n))
         return out
 

@@ -24,8 +24,8 @@ LIB = os.path.join(PKG, "libsilvan_b200.so")
 BIN = os.path.join(PKG, "bin", "silvan")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-SOURCES = ["graph_host.cpp", "gen.cpp", "sampler.cu", "counters.cu", "engine.cu", "server.cu",
-           "capi.cu"]
+SOURCES = ["graph_host.cpp", "gen.cpp", "graph_dev.cu", "sampler.cu", "counters.cu", "engine.cu",
+           "server.cu", "capi.cu"]
 
 
 def _nvcc():

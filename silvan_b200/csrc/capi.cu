@@ -118,6 +118,20 @@ int silvan_graph_upload(uint32_t n, int directed, const uint64_t *out_off,
     if (rc) return rc;
     silvan_graph_s *G = new (std::nothrow) silvan_graph_s();
     if (!G) return SILVAN_E_OOM;
+    if (cc) {
+        // the caller's arrays go to the device as they are (validated there)
+        G->g.ncomp = n_components;
+        G->g.diameter = diameter;
+        G->g.diameter_seconds = 0;
+        rc = G->g.upload_raw(n, directed != 0, out_off, out_adj, in_off, in_adj, cc);
+        if (rc != SILVAN_OK) {
+            delete G;
+            return rc;
+        }
+        *out = G;
+        return SILVAN_OK;
+    }
+    // components and the diameter bound are computed on the host
     HostGraph &h = G->g.host;
     h.n = n;
     h.directed = directed != 0;
@@ -135,12 +149,7 @@ int silvan_graph_upload(uint32_t n, int directed, const uint64_t *out_off,
                 return SILVAN_E_BADARG;
             }
     }
-    if (cc) {
-        G->g.cc.assign(cc, cc + n);
-        G->g.ncomp = n_components;
-        G->g.diameter = diameter;
-    }
-    return finish_graph(G, cc != nullptr, out);
+    return finish_graph(G, false, out);
 }
 
 int silvan_graph_from_pairs(const uint32_t *pairs, uint64_t count, int directed,
@@ -278,11 +287,11 @@ int silvan_graph_info(silvan_graph_t g, silvan_graph_info_t *info) {
         set_error("null argument");
         return SILVAN_E_BADARG;
     }
-    info->n = g->g.host.n;
+    info->n = g->g.n;
     info->n_components = g->g.ncomp;
-    info->m = g->g.host.num_edges();
+    info->m = g->g.m;
     info->diameter = g->g.diameter;
-    info->directed = g->g.host.directed ? 1 : 0;
+    info->directed = g->g.directed ? 1 : 0;
     return SILVAN_OK;
 }
 
@@ -292,17 +301,43 @@ int silvan_graph_csr(silvan_graph_t g, uint64_t *out_off, uint32_t *out_adj, uin
         set_error("null argument");
         return SILVAN_E_BADARG;
     }
-    const HostGraph &h = g->g.host;
-    if (out_off) std::copy(h.out_off.begin(), h.out_off.end(), out_off);
-    if (out_adj) std::copy(h.out_adj.begin(), h.out_adj.end(), out_adj);
-    const uint64_t *io = h.in_offsets();
-    if (in_off) std::copy(io, io + h.n + 1, in_off);
-    if (in_adj) {
-        const uint32_t *ia = h.in_neighbours();
-        std::copy(ia, ia + io[h.n], in_adj);
+    const DeviceGraph &G = g->g;
+    const uint32_t n = G.n;
+    if (G.has_host) {
+        const HostGraph &h = G.host;
+        if (out_off) std::copy(h.out_off.begin(), h.out_off.end(), out_off);
+        if (out_adj) std::copy(h.out_adj.begin(), h.out_adj.end(), out_adj);
+        const uint64_t *io = h.in_offsets();
+        if (in_off) std::copy(io, io + h.n + 1, in_off);
+        if (in_adj) {
+            const uint32_t *ia = h.in_neighbours();
+            std::copy(ia, ia + io[h.n], in_adj);
+        }
+        if (cc) std::copy(G.cc.begin(), G.cc.end(), cc);
+        return SILVAN_OK;
     }
-    if (cc) std::copy(g->g.cc.begin(), g->g.cc.end(), cc);
-    return SILVAN_OK;
+    // uploaded from caller arrays: read the device copy back
+    std::vector<uint32_t> off32(n + 1);
+    auto get = [&](const uint32_t *doff, const uint32_t *dadj, uint64_t cnt, uint64_t *off,
+                   uint32_t *adj) -> int {
+        if (off) {
+            if (cudaMemcpy(off32.data(), doff, sizeof(uint32_t) * (n + 1),
+                           cudaMemcpyDeviceToHost) != cudaSuccess)
+                return SILVAN_E_CUDA;
+            for (uint32_t i = 0; i <= n; i++) off[i] = off32[i];
+        }
+        if (adj && cnt &&
+            cudaMemcpy(adj, dadj, sizeof(uint32_t) * cnt, cudaMemcpyDeviceToHost) != cudaSuccess)
+            return SILVAN_E_CUDA;
+        return SILVAN_OK;
+    };
+    int rc = get(G.d_out_off, G.d_out_adj, G.m, out_off, out_adj);
+    if (rc == SILVAN_OK) rc = get(G.d_in_off, G.d_in_adj, G.m_in, in_off, in_adj);
+    if (rc == SILVAN_OK && cc &&
+        cudaMemcpy(cc, G.d_cc, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost) != cudaSuccess)
+        rc = SILVAN_E_CUDA;
+    if (rc != SILVAN_OK) set_error("device read failed");
+    return rc;
 }
 
 int silvan_graph_destroy(silvan_graph_t g) {

@@ -7,9 +7,11 @@
 #include <cstring>
 #include <iomanip>
 #include <map>
+#include <mutex>
 #include <sstream>
 
 #include "bounds.h"
+#include "graph_dev.cuh"
 
 namespace silvan {
 
@@ -87,6 +89,11 @@ double now_seconds() {
 // ---------------------------------------------------------------------------
 int DeviceGraph::upload() {
     const HostGraph &h = host;
+    has_host = true;
+    n = h.n;
+    directed = h.directed;
+    m = h.num_edges();
+    m_in = h.directed ? h.in_adj.size() : m;
     if (h.n < 2) {
         set_error("graph needs at least two nodes");
         return SILVAN_E_BADARG;
@@ -96,7 +103,6 @@ int DeviceGraph::upload() {
         return SILVAN_E_BADARG;
     }
     CK(cudaGetDevice(&device));
-    const uint32_t n = h.n;
     std::vector<uint32_t> off32(n + 1);
     auto put = [&](uint32_t **doff, uint32_t **dadj, const std::vector<uint64_t> &off,
                    const std::vector<uint32_t> &adj) -> int {
@@ -121,9 +127,67 @@ int DeviceGraph::upload() {
     return SILVAN_OK;
 }
 
+int DeviceGraph::upload_raw(uint32_t nn, bool dir, const uint64_t *out_off,
+                            const uint32_t *out_adj, const uint64_t *in_off,
+                            const uint32_t *in_adj, const uint32_t *cc_in) {
+    has_host = false;
+    n = nn;
+    directed = dir;
+    m = out_off[nn];
+    m_in = dir ? in_off[nn] : m;
+    if (nn < 2) {
+        set_error("graph needs at least two nodes");
+        return SILVAN_E_BADARG;
+    }
+    if (m >= 0xffffffffull || m_in >= 0xffffffffull) {
+        set_error("graphs with 2^32 or more edge entries are not supported");
+        return SILVAN_E_BADARG;
+    }
+    CK(cudaGetDevice(&device));
+    uint64_t *tmp = nullptr;
+    uint32_t *bad = nullptr;
+    RK(dmalloc(&tmp, (size_t)nn + 1));
+    RK(dmalloc(&bad, 1));
+    auto put = [&](uint32_t **doff, uint32_t **dadj, const uint64_t *off, const uint32_t *adj,
+                   uint64_t cnt) -> int {
+        RK(dmalloc(doff, (size_t)nn + 1));
+        RK(dmalloc(dadj, cnt));
+        CK(cudaMemcpy(tmp, off, sizeof(uint64_t) * (nn + 1), cudaMemcpyHostToDevice));
+        CK(narrow_offsets(tmp, *doff, nn + 1, 0));
+        if (cnt) CK(cudaMemcpy(*dadj, adj, sizeof(uint32_t) * cnt, cudaMemcpyHostToDevice));
+        CK(validate_rows(*doff, *dadj, nn, bad, 0));
+        return SILVAN_OK;
+    };
+    CK(cudaMemset(bad, 0, sizeof(uint32_t)));
+    int rc = put(&d_out_off, &d_out_adj, out_off, out_adj, m);
+    if (rc == SILVAN_OK) {
+        if (dir) {
+            rc = put(&d_in_off, &d_in_adj, in_off, in_adj, m_in);
+        } else {
+            d_in_off = d_out_off;
+            d_in_adj = d_out_adj;
+        }
+    }
+    if (rc == SILVAN_OK) rc = dmalloc(&d_cc, nn);
+    if (rc == SILVAN_OK)
+        rc = cuda_status(cudaMemcpy(d_cc, cc_in, sizeof(uint32_t) * nn, cudaMemcpyHostToDevice),
+                         "cc upload");
+    uint32_t hbad = 0;
+    if (rc == SILVAN_OK)
+        rc = cuda_status(cudaMemcpy(&hbad, bad, sizeof(uint32_t), cudaMemcpyDeviceToHost),
+                         "validation");
+    dfree(tmp);
+    dfree(bad);
+    if (rc == SILVAN_OK && hbad) {
+        set_error("CSR rows must hold ascending unique ids < n");
+        rc = SILVAN_E_BADARG;
+    }
+    return rc;
+}
+
 uint64_t DeviceGraph::device_bytes() const {
-    uint64_t b = 4ull * (host.n + 1) + 4ull * host.num_edges() + 4ull * host.n;
-    if (host.directed) b += 4ull * (host.n + 1) + 4ull * host.in_adj.size();
+    uint64_t b = 4ull * (n + 1) + 4ull * m + 4ull * n;
+    if (directed) b += 4ull * (n + 1) + 4ull * m_in;
     return b;
 }
 
@@ -246,8 +310,8 @@ int Engine::round(const std::vector<Job *> &jobs, const std::vector<JobRequest> 
         S.in_off = G.d_in_off;
         S.in_adj = G.d_in_adj;
         S.cc = G.d_cc;
-        S.n = G.host.n;
-        S.directed = G.host.directed ? 1 : 0;
+        S.n = G.n;
+        S.directed = G.directed ? 1 : 0;
         S.seed = job->params().seed;
         S.alpha = job->alpha();
         S.np_cap = job->params().np_cap;
@@ -267,7 +331,7 @@ int Engine::round(const std::vector<Job *> &jobs, const std::vector<JobRequest> 
     uint32_t total = 0;
     for (uint32_t s = 0; s < idx.size(); s++) {
         const JobRequest &r = reqs[idx[s]];
-        if (r.count > kRoundSamples || jobs[idx[s]]->graph()->host.n > slots_.n) {
+        if (r.count > kRoundSamples || jobs[idx[s]]->graph()->n > slots_.n) {
             set_error("request larger than the round buffers or graph larger than the slots");
             return SILVAN_E_BADARG;
         }
@@ -345,13 +409,96 @@ int Engine::round(const std::vector<Job *> &jobs, const std::vector<JobRequest> 
 }
 
 // ---------------------------------------------------------------------------
+// Engine pool
+// ---------------------------------------------------------------------------
+namespace {
+struct PooledEngine {
+    int device;
+    uint32_t requested_slots;
+    Engine *eng;
+};
+std::mutex g_pool_mu;
+std::vector<PooledEngine> g_pool_free;
+std::vector<PooledEngine> g_pool_busy;
+}  // namespace
+
+Engine *engine_acquire(uint64_t n, uint32_t slots, int *rc) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    {
+        std::lock_guard<std::mutex> lk(g_pool_mu);
+        for (size_t i = 0; i < g_pool_free.size(); i++) {
+            PooledEngine &p = g_pool_free[i];
+            if (p.device == dev && p.eng->n_max() >= n && p.requested_slots == slots) {
+                PooledEngine q = p;
+                g_pool_free.erase(g_pool_free.begin() + i);
+                g_pool_busy.push_back(q);
+                *rc = SILVAN_OK;
+                return q.eng;
+            }
+        }
+    }
+    Engine *e = new Engine();
+    *rc = e->init(n, slots, 0);
+    if (*rc != SILVAN_OK) {
+        // release idle engines of this device and try once more
+        std::vector<Engine *> drop;
+        {
+            std::lock_guard<std::mutex> lk(g_pool_mu);
+            for (size_t i = 0; i < g_pool_free.size();)
+                if (g_pool_free[i].device == dev) {
+                    drop.push_back(g_pool_free[i].eng);
+                    g_pool_free.erase(g_pool_free.begin() + i);
+                } else {
+                    i++;
+                }
+        }
+        for (Engine *d : drop) delete d;
+        delete e;
+        e = new Engine();
+        *rc = e->init(n, slots, 0);
+        if (*rc != SILVAN_OK) {
+            delete e;
+            return nullptr;
+        }
+    }
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    g_pool_busy.push_back(PooledEngine{dev, slots, e});
+    return e;
+}
+
+void engine_release(Engine *e) {
+    if (!e) return;
+    cudaStreamSynchronize(e->stream());
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    for (size_t i = 0; i < g_pool_busy.size(); i++)
+        if (g_pool_busy[i].eng == e) {
+            g_pool_free.push_back(g_pool_busy[i]);
+            g_pool_busy.erase(g_pool_busy.begin() + i);
+            return;
+        }
+}
+
+int Job::borrow_engine() {
+    if (own_engine_) return SILVAN_OK;
+    int rc = SILVAN_OK;
+    own_engine_ = engine_acquire(n_, p_.slots, &rc);
+    return rc;
+}
+
+void Job::return_engine() {
+    if (!own_engine_) return;
+    engine_release(own_engine_);
+    own_engine_ = nullptr;
+}
+
+// ---------------------------------------------------------------------------
 // Job: allocation and commit
 // ---------------------------------------------------------------------------
 Job::~Job() {
-    if (stream_) cudaStreamSynchronize(stream_);
+    if (own_engine_) cudaStreamSynchronize(own_engine_->stream());
     if (apply_graph_) cudaGraphExecDestroy(apply_graph_);
-    delete own_engine_;
-    own_engine_ = nullptr;
+    return_engine();
     stream_ = nullptr;
     RoundBuffers &r = rb_;
     dfree(r.pl);
@@ -435,7 +582,7 @@ uint64_t Job::device_bytes() const {
 }
 
 int Job::init() {
-    n_ = g_->host.n;
+    n_ = g_->n;
     if (!(p_.eps > 0 && p_.eps < 1) || !(p_.delta > 0 && p_.delta < 1)) {
         set_error("eps and delta must lie in (0, 1)");
         return SILVAN_E_BADARG;
@@ -874,7 +1021,7 @@ int Job::begin(FILE *sink, cudaStream_t stream) {
     }
     sink_ = sink;
     stream_ = stream;
-    const uint64_t m = g_->host.num_edges();
+    const uint64_t m = g_->m;
     const int D = (int)g_->diameter;
     const double eps = p_.eps, delta = p_.delta;
     absolute_ = p_.k == 0;
@@ -1207,11 +1354,11 @@ int Job::finish(silvan_result_t *res) {
 }
 
 int Job::run(silvan_result_t *res, FILE *sink) {
-    if (!own_engine_) {
-        own_engine_ = new Engine();
-        int rc = own_engine_->init(n_, p_.slots, 0);
-        if (rc != SILVAN_OK) return rc;
-    }
+    RK(borrow_engine());
+    struct Return {
+        Job *j;
+        ~Return() { j->return_engine(); }
+    } ret{this};
     own_engine_->reset_timers();
     launches = 0;
     RK(begin(sink, own_engine_->stream()));
@@ -1233,11 +1380,18 @@ int Job::run(silvan_result_t *res, FILE *sink) {
 }
 
 int Job::step(uint32_t rounds, silvan_status_t *st, FILE *sink) {
-    if (!own_engine_) {
-        own_engine_ = new Engine();
-        int rc = own_engine_->init(n_, p_.slots, 0);
-        if (rc != SILVAN_OK) return rc;
+    if (phase_ == kDone) {
+        if (st) {
+            st->samples = result_.num_samples;
+            st->void_samples = result_.void_samples;
+            st->vis_edges = result_.vis_edges;
+            st->backtracked_paths = result_.backtracked_paths;
+            st->pass = 2;
+            st->done = 1;
+        }
+        return SILVAN_OK;
     }
+    RK(borrow_engine());
     if (phase_ == kInit) {
         own_engine_->reset_timers();
         launches = 0;
@@ -1267,6 +1421,7 @@ int Job::step(uint32_t rounds, silvan_status_t *st, FILE *sink) {
         st->pass = phase_ == kPass1 ? 1 : 2;
         st->done = done() ? 1 : 0;
     }
+    if (done()) return_engine();
     return SILVAN_OK;
 }
 
@@ -1363,11 +1518,11 @@ int Job::read_topk(uint32_t *nodes, double *values, uint32_t cap, uint32_t *coun
 int Job::replay(uint32_t first, uint32_t count, double alpha, std::vector<int32_t> &pl,
                 std::vector<int32_t> &np, std::vector<uint64_t> &vis,
                 std::vector<int32_t> &status, std::vector<PathRec> &recs) {
-    if (!own_engine_) {
-        own_engine_ = new Engine();
-        int rc = own_engine_->init(n_, p_.slots, 0);
-        if (rc != SILVAN_OK) return rc;
-    }
+    RK(borrow_engine());
+    struct Return {
+        Job *j;
+        ~Return() { j->return_engine(); }
+    } ret{this};
     stream_ = own_engine_->stream();
     pl.assign(count, 0);
     np.assign(count, 0);

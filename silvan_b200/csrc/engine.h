@@ -27,6 +27,13 @@ int cuda_status(cudaError_t e, const char *what);
 double now_seconds();
 
 struct DeviceGraph {
+    // metadata (always set once uploaded)
+    uint32_t n = 0;
+    bool directed = false;
+    uint64_t m = 0;     // out-edge entries (edges_num of the reference)
+    uint64_t m_in = 0;  // in-edge entries (directed graphs)
+    // host copy, kept when the graph was built on the host (file or pairs)
+    bool has_host = false;
     HostGraph host;
     std::vector<uint32_t> cc;
     uint32_t ncomp = 0;
@@ -38,7 +45,11 @@ struct DeviceGraph {
     uint32_t *d_cc = nullptr;
     int device = 0;
 
-    int upload();
+    int upload();  // from `host` and `cc`
+    // from caller-owned host arrays (ideally pinned): copied straight to the
+    // device, offsets narrowed and rows validated there
+    int upload_raw(uint32_t n, bool directed, const uint64_t *out_off, const uint32_t *out_adj,
+                   const uint64_t *in_off, const uint32_t *in_adj, const uint32_t *cc);
     uint64_t device_bytes() const;
     ~DeviceGraph();
 };
@@ -65,6 +76,12 @@ struct JobRequest {
 };
 
 class Job;
+class Engine;
+
+// Process-wide pool of sampler engines per device: a job borrows one for its
+// run, so repeated jobs do not re-allocate and re-initialise the slots.
+Engine *engine_acquire(uint64_t n, uint32_t slots, int *rc);
+void engine_release(Engine *e);
 
 class Engine {
   public:
@@ -169,7 +186,9 @@ class Job {
 
     DeviceGraph *g_;
     silvan_params_t p_;
-    Engine *own_engine_ = nullptr;
+    Engine *own_engine_ = nullptr;  // borrowed from the pool while running
+    int borrow_engine();
+    void return_engine();
     cudaStream_t stream_ = nullptr;  // stream of the engine driving the job
     RoundBuffers rb_{};
     uint32_t n_ = 0;

@@ -1,0 +1,43 @@
+// Device-side CSR preparation (see graph_dev.cuh).
+#include "graph_dev.cuh"
+
+namespace silvan {
+
+namespace {
+
+__global__ void narrow_offsets_kernel(const uint64_t *in, uint32_t *out, uint32_t count) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count;
+         i += gridDim.x * blockDim.x)
+        out[i] = (uint32_t)in[i];
+}
+
+// one warp per row
+__global__ void validate_rows_kernel(const uint32_t *off, const uint32_t *adj, uint32_t n,
+                                     uint32_t *bad) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < n; v += nw) {
+        const uint32_t b = off[v], e = off[v + 1];
+        bool ok = e >= b;
+        for (uint32_t k = b + lane; ok && k < e; k += 32) {
+            const uint32_t y = adj[k];
+            if (y >= n || (k > b && adj[k - 1] >= y)) ok = false;
+        }
+        if (__any_sync(0xffffffffu, !ok) && lane == 0) atomicOr(bad, 1u);
+    }
+}
+
+}  // namespace
+
+cudaError_t narrow_offsets(const uint64_t *in, uint32_t *out, uint32_t count, cudaStream_t s) {
+    narrow_offsets_kernel<<<592, 256, 0, s>>>(in, out, count);
+    return cudaGetLastError();
+}
+
+cudaError_t validate_rows(const uint32_t *off, const uint32_t *adj, uint32_t n, uint32_t *bad,
+                          cudaStream_t s) {
+    validate_rows_kernel<<<1184, 256, 0, s>>>(off, adj, n, bad);
+    return cudaGetLastError();
+}
+
+}  // namespace silvan

@@ -151,8 +151,8 @@ struct Server {
     void finish(ServerRequest *r, int rc) {
         if (rc == SILVAN_OK && r->job) {
             r->job->finish(&r->result);
-            r->estimates.resize(r->graph->host.n);
-            r->job->read_estimates(r->estimates.data(), r->graph->host.n);
+            r->estimates.resize(r->graph->n);
+            r->job->read_estimates(r->estimates.data(), r->graph->n);
             if (r->params.k > 0) {
                 uint32_t cap = r->result.numresults_topk + 1, cnt = 0;
                 r->topk_nodes.resize(cap);
