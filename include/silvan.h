@@ -278,6 +278,29 @@ int silvan_replay_samples(silvan_graph_t g, uint64_t seed, uint32_t first, uint3
                           int32_t *sample_status, uint32_t *ent_node, int32_t *ent_cnt,
                           uint64_t ent_cap, uint64_t *ent_total);
 
+/* No counterpart in the reference.  The same per-sample sampler as
+ * silvan_replay_samples, for callers that cannot allocate device memory:
+ * code that records work into a CUDA graph replayed later, a process that
+ * already holds its whole memory quota, or a runtime that hands the library
+ * only pre-allocated buffers.  It calls no cudaMalloc/cudaFree: the sampler's
+ * scratch is a fixed 64 MiB static device array (held by every GPU that loads
+ * the library until exit), which limits a call to graphs of about 1.4 million
+ * nodes and to 65536 samples (SILVAN_E_CAPACITY beyond).  Every output is a
+ * DEVICE buffer supplied by the caller; d_records receives (node, sample,
+ * count) triples, unordered, and *d_record_count their number (when it
+ * exceeds record_cap the surplus is dropped and the affected samples carry
+ * SILVAN_E_CAPACITY).  The work is queued on `stream` (a cudaStream_t, NULL
+ * for the default stream); outputs are ready when the stream reaches it.  The
+ * first call on a device looks up the scratch's device address and should
+ * come before any stream capture.  All calls share the scratch, so calls that
+ * overlap on the GPU race. */
+int silvan_replay_samples_noalloc(silvan_graph_t g, uint64_t seed, uint32_t first,
+                                  uint32_t count, double alpha, uint32_t np_cap,
+                                  int32_t *d_path_length, int32_t *d_num_paths,
+                                  uint64_t *d_vis_edges, int32_t *d_status,
+                                  uint32_t *d_records, uint64_t record_cap,
+                                  unsigned long long *d_record_count, void *stream);
+
 /* ---- synthetic workloads --------------------------------------------------- */
 
 /* Generators of the measured workloads; they write at most cap (u, v) pairs

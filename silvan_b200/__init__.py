@@ -36,7 +36,7 @@ EXPORTS = [
     "silvan_graph_from_pairs", "silvan_last_error", "silvan_version", "silvan_job_result",
     "silvan_jobs_run_batched", "silvan_server_create", "silvan_server_submit",
     "silvan_server_poll", "silvan_server_wait", "silvan_server_estimates", "silvan_server_stats",
-    "silvan_server_destroy",
+    "silvan_server_destroy", "silvan_replay_samples_noalloc",
 ]
 
 REQ_QUEUED, REQ_RUNNING, REQ_DONE = 1, 2, 3
@@ -134,6 +134,9 @@ def load(path: str = LIB_PATH):
         "silvan_server_estimates": (C.c_int, [P, C.c_uint64, P, C.c_uint32, P, P, C.c_uint32, P]),
         "silvan_server_stats": (C.c_int, [P, P]),
         "silvan_server_destroy": (C.c_int, [P]),
+        "silvan_replay_samples_noalloc": (C.c_int, [P, C.c_uint64, C.c_uint32, C.c_uint32,
+                                                    C.c_double, C.c_uint32, P, P, P, P, P,
+                                                    C.c_uint64, P, P]),
         "silvan_last_error": (C.c_char_p, []),
         "silvan_version": (C.c_char_p, []),
     }

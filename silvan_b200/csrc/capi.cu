@@ -12,6 +12,11 @@
 
 namespace silvan {
 const char *last_error_cstr();
+int replay_samples_noalloc(const DeviceGraph &G, uint64_t seed, uint32_t first, uint32_t count,
+                           double alpha, uint32_t np_cap, int32_t *d_path_length,
+                           int32_t *d_num_paths, uint64_t *d_vis_edges, int32_t *d_status,
+                           uint32_t *d_records, uint64_t record_cap,
+                           unsigned long long *d_record_count, cudaStream_t stream);
 }
 
 struct silvan_graph_s {
@@ -549,6 +554,21 @@ int silvan_replay_samples(silvan_graph_t g, uint64_t seed, uint32_t first, uint3
         if (ent_cnt) ent_cnt[i] = (int32_t)recs[i].count;
     }
     return SILVAN_OK;
+}
+
+int silvan_replay_samples_noalloc(silvan_graph_t g, uint64_t seed, uint32_t first,
+                                  uint32_t count, double alpha, uint32_t np_cap,
+                                  int32_t *d_path_length, int32_t *d_num_paths,
+                                  uint64_t *d_vis_edges, int32_t *d_status,
+                                  uint32_t *d_records, uint64_t record_cap,
+                                  unsigned long long *d_record_count, void *stream) {
+    if (!g) {
+        set_error("null graph");
+        return SILVAN_E_BADARG;
+    }
+    return replay_samples_noalloc(g->g, seed, first, count, alpha, np_cap, d_path_length,
+                                  d_num_paths, d_vis_edges, d_status, d_records, record_cap,
+                                  d_record_count, (cudaStream_t)stream);
 }
 
 int silvan_generate(int kind, uint32_t a, uint32_t b, uint32_t c, double x, double y,
