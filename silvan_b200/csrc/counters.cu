@@ -181,6 +181,7 @@ __device__ void fold_node(const RoundBuffers &rb, const JobCounters &jc, const A
         if (pass2) m = jc.mcrade[(uint64_t)node * kTrials + lane];
     } else if (lane == 25) {
         acc = jc.approx[node];
+        lu = jc.last_upd[node];
     } else if (lane == 26) {
         acc = jc.wimpy[node];
     }
@@ -231,7 +232,10 @@ __device__ void fold_node(const RoundBuffers &rb, const JobCounters &jc, const A
         if (pass2) jc.mcrade[(uint64_t)node * kTrials + lane] = m;
     } else if (lane == 25) {
         jc.approx[node] = acc;
-        if (lu) jc.last_upd[node] = lu;
+        if (lu) {
+            if (jc.last_upd[node] == 0) jc.upd_list[atomicAdd(&jc.sc->n_upd, 1u)] = node;
+            jc.last_upd[node] = lu;
+        }
         atomic_max_nonneg_double(&jc.sc->sup_approx_bits, acc);
     } else if (lane == 26) {
         jc.wimpy[node] = acc;
@@ -374,37 +378,47 @@ __global__ void reset_touched_kernel(const ApplyState *st) {
 
 __global__ void stop_init_kernel(StopReduction *out, int nparts, long long init) {
     for (int i = threadIdx.x; i < nparts * kTrials; i += blockDim.x) out->mc_max[i] = init;
-    for (int i = threadIdx.x; i < nparts; i += blockDim.x) out->wimpy_max[i] = 0.0;
+    for (int i = threadIdx.x; i < nparts; i += blockDim.x) {
+        out->wimpy_max[i] = 0.0;
+        out->touched[i] = 0;
+    }
     if (threadIdx.x == 0) {
         out->approx_max = 0.0;
         out->wimpy_all_max = 0.0;
     }
 }
 
-__global__ void __launch_bounds__(512) stop_reduce_kernel(JobCounters jc, uint32_t n, int nparts,
+// One warp per updated node: lanes 0..24 read the node's 25 trials (one
+// 200-byte row), lane 25 approx and wimpy.
+__global__ void __launch_bounds__(512) stop_reduce_kernel(JobCounters jc, int nparts,
                                                           long long init, StopReduction *out) {
     __shared__ long long smc[kMaxPartitions * kTrials];
     __shared__ unsigned long long sw[kMaxPartitions];
+    __shared__ uint32_t st[kMaxPartitions];
     for (int i = threadIdx.x; i < nparts * kTrials; i += blockDim.x) smc[i] = init;
-    for (int i = threadIdx.x; i < nparts; i += blockDim.x) sw[i] = 0ull;
-    __syncthreads();
-    const uint64_t total = (uint64_t)n * kTrials;
-    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < total; i += stride) {
-        const uint32_t v = (uint32_t)(i / kTrials);
-        const uint32_t j = (uint32_t)(i - (uint64_t)v * kTrials);
-        const int p = jc.partition[v];
-        const long long m = jc.mcrade[i];
-        if (m > smc[p * kTrials + j]) atomicMax(&smc[p * kTrials + j], m);
+    for (int i = threadIdx.x; i < nparts; i += blockDim.x) {
+        sw[i] = 0ull;
+        st[i] = 0;
     }
+    __syncthreads();
+    const uint32_t T = jc.sc->n_upd;
+    const int lane = threadIdx.x & 31;
+    const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
     unsigned long long amax = 0, wmax = 0;
-    for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < n; v += stride) {
-        const unsigned long long wb = (unsigned long long)__double_as_longlong(jc.wimpy[v]);
-        const unsigned long long ab = (unsigned long long)__double_as_longlong(jc.approx[v]);
+    for (uint32_t t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < T; t += nw) {
+        const uint32_t v = jc.upd_list[t];
         const int p = jc.partition[v];
-        if (wb > sw[p]) atomicMax(&sw[p], wb);
-        amax = ab > amax ? ab : amax;
-        wmax = wb > wmax ? wb : wmax;
+        if (lane < kTrials) {
+            const long long m = jc.mcrade[(uint64_t)v * kTrials + lane];
+            if (m > smc[p * kTrials + lane]) atomicMax(&smc[p * kTrials + lane], m);
+        } else if (lane == kTrials) {
+            const unsigned long long wb = (unsigned long long)__double_as_longlong(jc.wimpy[v]);
+            const unsigned long long ab = (unsigned long long)__double_as_longlong(jc.approx[v]);
+            if (wb > sw[p]) atomicMax(&sw[p], wb);
+            atomicAdd(&st[p], 1u);
+            amax = ab > amax ? ab : amax;
+            wmax = wb > wmax ? wb : wmax;
+        }
     }
     for (int o = 16; o > 0; o >>= 1) {
         unsigned long long x = __shfl_xor_sync(0xffffffffu, amax, o);
@@ -412,15 +426,17 @@ __global__ void __launch_bounds__(512) stop_reduce_kernel(JobCounters jc, uint32
         amax = x > amax ? x : amax;
         wmax = y > wmax ? y : wmax;
     }
-    if ((threadIdx.x & 31) == 0) {
-        atomicMax(reinterpret_cast<unsigned long long *>(&out->approx_max), amax);
-        atomicMax(reinterpret_cast<unsigned long long *>(&out->wimpy_all_max), wmax);
+    if (lane == 0) {
+        if (amax) atomicMax(reinterpret_cast<unsigned long long *>(&out->approx_max), amax);
+        if (wmax) atomicMax(reinterpret_cast<unsigned long long *>(&out->wimpy_all_max), wmax);
     }
     __syncthreads();
     for (int i = threadIdx.x; i < nparts * kTrials; i += blockDim.x)
         if (smc[i] != init) atomicMax(&out->mc_max[i], smc[i]);
-    for (int i = threadIdx.x; i < nparts; i += blockDim.x)
+    for (int i = threadIdx.x; i < nparts; i += blockDim.x) {
         if (sw[i]) atomicMax(reinterpret_cast<unsigned long long *>(&out->wimpy_max[i]), sw[i]);
+        if (st[i]) atomicAdd(&out->touched[i], st[i]);
+    }
 }
 
 __global__ void peel_index_kernel(JobCounters jc, uint32_t n, double m, double a, uint32_t *unc,
@@ -441,8 +457,24 @@ __global__ void peel_index_kernel(JobCounters jc, uint32_t n, double m, double a
     }
 }
 
+// Shared-memory histogram per block (the bins are few: about log(m)/log(a)).
 __global__ void peel_hist_kernel(JobCounters jc, uint32_t n, int32_t idx_min, int32_t nbins,
                                  uint32_t *hist) {
+    extern __shared__ uint32_t sh[];
+    for (int i = threadIdx.x; i < nbins; i += blockDim.x) sh[i] = 0;
+    __syncthreads();
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+        int32_t b = jc.peel_idx[v] - idx_min;
+        b = b < 0 ? 0 : (b >= nbins ? nbins - 1 : b);
+        atomicAdd(&sh[b], 1u);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < nbins; i += blockDim.x)
+        if (sh[i]) atomicAdd(&hist[i], sh[i]);
+}
+
+__global__ void peel_hist_global_kernel(JobCounters jc, uint32_t n, int32_t idx_min,
+                                        int32_t nbins, uint32_t *hist) {
     for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
         int32_t b = jc.peel_idx[v] - idx_min;
         b = b < 0 ? 0 : (b >= nbins ? nbins - 1 : b);
@@ -481,10 +513,10 @@ cudaError_t apply_round(const ApplyState *st, uint32_t *n_touched, cudaStream_t 
     return cudaGetLastError();
 }
 
-cudaError_t stop_reduce(const JobCounters &jc, uint32_t n, int nparts, long long init,
+cudaError_t stop_reduce(const JobCounters &jc, int nparts, long long init,
                         StopReduction *out_dev, cudaStream_t stream) {
     stop_init_kernel<<<1, 256, 0, stream>>>(out_dev, nparts, init);
-    stop_reduce_kernel<<<296, 512, 0, stream>>>(jc, n, nparts, init, out_dev);
+    stop_reduce_kernel<<<296, 512, 0, stream>>>(jc, nparts, init, out_dev);
     return cudaGetLastError();
 }
 
@@ -499,7 +531,11 @@ cudaError_t peel_index(const JobCounters &jc, uint32_t n, double num_samples, do
 cudaError_t peel_hist(const JobCounters &jc, uint32_t n, int32_t idx_min, int32_t nbins,
                       uint32_t *hist, cudaStream_t stream) {
     cudaMemsetAsync(hist, 0, sizeof(uint32_t) * nbins, stream);
-    peel_hist_kernel<<<592, 256, 0, stream>>>(jc, n, idx_min, nbins, hist);
+    if (nbins <= 8192)
+        peel_hist_kernel<<<296, 512, sizeof(uint32_t) * nbins, stream>>>(jc, n, idx_min, nbins,
+                                                                          hist);
+    else
+        peel_hist_global_kernel<<<592, 256, 0, stream>>>(jc, n, idx_min, nbins, hist);
     return cudaGetLastError();
 }
 

@@ -25,6 +25,8 @@ struct JobScalars {
     unsigned long long pred_entries;     // predecessor entries recorded
     int32_t error;                       // first SILVAN_E_* seen
     uint32_t n_cross;                    // crossings of the top-k "approx >= 3" mark
+    uint32_t n_upd;                      // entries of upd_list
+    uint32_t pad;
 };
 
 struct RoundBuffers {
@@ -62,6 +64,7 @@ struct JobCounters {
     JobScalars *sc;
     int32_t *partition;   // dense partition id per node
     int32_t *peel_idx;    // raw peeling index per node
+    uint32_t *upd_list;   // nodes updated since the counters were last reset
 };
 
 struct ApplyArgs {
@@ -97,13 +100,17 @@ cudaError_t apply_init();
 // Reduction for one stopping-rule evaluation: per partition and trial the
 // maximum of mcrade (initialised to -n_pairs), per partition the maximum of
 // emp_wimpy_vars, and the global maxima of approx and emp_wimpy_vars.
+// Only the nodes on upd_list are read: every other node still has
+// approx = wimpy = mcrade = 0, which the host folds in per partition from
+// touched[] (a partition with fewer touched nodes than members has zeros).
 struct StopReduction {
     long long mc_max[kMaxPartitions * kTrials];
     double wimpy_max[kMaxPartitions];
+    uint32_t touched[kMaxPartitions];
     double approx_max;
     double wimpy_all_max;
 };
-cudaError_t stop_reduce(const JobCounters &jc, uint32_t n, int nparts, long long init,
+cudaError_t stop_reduce(const JobCounters &jc, int nparts, long long init,
                         StopReduction *out_dev, cudaStream_t stream);
 
 // Empirical peeling index of every node (Probabilistic.cpp:855-862), with the

@@ -253,6 +253,12 @@ Engine::~Engine() {
 
 int Engine::init(uint64_t n_max, uint32_t slots, uint64_t mem_budget) {
     CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    {
+        int dev = 0, khz = 0;
+        CK(cudaGetDevice(&dev));
+        CK(cudaDeviceGetAttribute(&khz, cudaDevAttrClockRate, dev));
+        clock_khz_ = khz;
+    }
     for (auto &e : ev_) CK(cudaEventCreate(&e));
     if (slots == 0) {
         int dev = 0, sms = 0;
@@ -292,11 +298,11 @@ int Engine::ensure_segs(uint32_t nsegs) {
 }
 
 int Engine::round(const std::vector<Job *> &jobs, const std::vector<JobRequest> &reqs,
-                  bool commit, std::vector<uint64_t> *records) {
+                  std::vector<uint64_t> &records) {
     std::vector<uint32_t> idx;
     for (uint32_t i = 0; i < jobs.size(); i++)
         if (reqs[i].count > 0) idx.push_back(i);
-    if (records) records->assign(jobs.size(), 0);
+    records.assign(jobs.size(), 0);
     if (idx.empty()) return SILVAN_OK;
     RK(ensure_segs((uint32_t)idx.size()));
     auto fill = [&](uint32_t s, uint32_t j, uint32_t base) {
@@ -341,6 +347,7 @@ int Engine::round(const std::vector<Job *> &jobs, const std::vector<JobRequest> 
     h_hdr_->nsegs = (uint32_t)idx.size();
     h_hdr_->total = total;
     h_hdr_->work = 0;
+    h_hdr_->cycles = 0;
     const uint32_t grid = std::min<uint32_t>(slots_.slots, total);
     for (;;) {
         CK(cudaMemcpyAsync(d_segs_, h_segs_, sizeof(SegDesc) * idx.size(),
@@ -373,10 +380,19 @@ int Engine::round(const std::vector<Job *> &jobs, const std::vector<JobRequest> 
         launches_ += 2;
         CK(cudaMemcpyAsync(h_cursors_, d_cursors_, sizeof(unsigned long long) * idx.size(),
                            cudaMemcpyDeviceToHost, stream_));
+        CK(cudaMemcpyAsync(h_hdr_, d_hdr_, sizeof(RoundHeader), cudaMemcpyDeviceToHost, stream_));
         CK(cudaStreamSynchronize(stream_));
         float ms = 0;
         cudaEventElapsedTime(&ms, ev_[0], ev_[1]);
         sample_ms_ += ms;
+        // cost model for speculative draws: a launch lasts about as long as
+        // its slowest sample, so the samples that fit into that time on the
+        // other slots cost (almost) nothing extra
+        if (h_hdr_->total > 0 && clock_khz_ > 0) {
+            const double cta_ms = (double)h_hdr_->cycles / clock_khz_ / h_hdr_->total;
+            cta_ms_per_sample_ = cta_ms_per_sample_ > 0 ? 0.5 * (cta_ms_per_sample_ + cta_ms) : cta_ms;
+            last_launch_ms_ = ms;
+        }
         bool redo = false;
         uint32_t base = 0;
         for (uint32_t s = 0; s < idx.size(); s++) {
@@ -392,20 +408,19 @@ int Engine::round(const std::vector<Job *> &jobs, const std::vector<JobRequest> 
         }
         if (!redo) break;
         // the path maps did not fit: redraw the round (deterministic)
+        h_hdr_->nsegs = (uint32_t)idx.size();
+        h_hdr_->total = total;
         h_hdr_->work = 0;
+        h_hdr_->cycles = 0;
     }
-    if (records)
-        for (uint32_t s = 0; s < idx.size(); s++) (*records)[idx[s]] = h_cursors_[s];
-    if (!commit) return SILVAN_OK;
-    CK(cudaEventRecord(ev_[2], stream_));
-    for (uint32_t s = 0; s < idx.size(); s++)
-        RK(jobs[idx[s]]->apply(reqs[idx[s]], (uint32_t)h_cursors_[s], stream_));
-    CK(cudaEventRecord(ev_[3], stream_));
-    CK(cudaEventSynchronize(ev_[3]));
-    float ms = 0;
-    cudaEventElapsedTime(&ms, ev_[2], ev_[3]);
-    apply_ms_ += ms;
+    for (uint32_t s = 0; s < idx.size(); s++) records[idx[s]] = h_cursors_[s];
     return SILVAN_OK;
+}
+
+uint32_t Engine::free_samples() const {
+    if (cta_ms_per_sample_ <= 0 || last_launch_ms_ <= 0) return 0;
+    const double f = last_launch_ms_ * slots_.slots / cta_ms_per_sample_;
+    return (uint32_t)std::min<double>(f, (double)kRoundSamples);
 }
 
 // ---------------------------------------------------------------------------
@@ -525,6 +540,7 @@ Job::~Job() {
     dfree(jc_.sc);
     dfree(jc_.partition);
     dfree(jc_.peel_idx);
+    dfree(jc_.upd_list);
     dfree(d_state_);
     dfree(d_red_);
     dfree(d_unc_);
@@ -535,6 +551,8 @@ Job::~Job() {
     hfree(h_red_);
     hfree(h_sc_);
     for (auto &e : ev_run_)
+        if (e) cudaEventDestroy(e);
+    for (auto &e : ev_commit_)
         if (e) cudaEventDestroy(e);
 }
 
@@ -589,6 +607,7 @@ int Job::init() {
     }
     if (p_.np_cap == 0) p_.np_cap = 1u << 24;
     for (auto &e : ev_run_) CK(cudaEventCreate(&e));
+    for (auto &e : ev_commit_) CK(cudaEventCreate(&e));
     RK(alloc_round(kRoundSamples, kInitialRecords));
     const uint32_t n = n_;
     RK(dmalloc(&jc_.approx, n));
@@ -601,6 +620,7 @@ int Job::init() {
     RK(dmalloc(&jc_.sc, 1));
     RK(dmalloc(&jc_.partition, n));
     RK(dmalloc(&jc_.peel_idx, n));
+    RK(dmalloc(&jc_.upd_list, n));
     RK(dmalloc(&d_state_, 1));
     RK(dmalloc(&d_red_, 1));
     RK(dmalloc(&d_unc_, kUncertainCap));
@@ -635,28 +655,30 @@ int Job::capture_apply(cudaStream_t stream) {
     return SILVAN_OK;
 }
 
-// Commits samples [r.first_global, +r.count) whose raw outputs the engine left
-// in rb_, in apply sub-rounds of at most kLargeBucket samples.
-int Job::apply(const JobRequest &r, uint32_t n_records, cudaStream_t stream) {
-    RK(capture_apply(stream));
-    for (uint32_t lo = 0; lo < r.count; lo += kLargeBucket) {
+// Commits samples [lo, hi) (indices into the drawn range r) whose raw outputs
+// the engine left in rb_, in apply sub-rounds of at most kLargeBucket samples.
+int Job::apply_range(const JobRequest &r, uint32_t lo, uint32_t hi, uint64_t n_records) {
+    RK(capture_apply(stream_));
+    for (uint32_t a0 = lo; a0 < hi; a0 += kLargeBucket) {
         ApplyState &st = h_state_[arg_slot_];
         arg_slot_ = (arg_slot_ + 1) % kArgRing;
         st.rb = rb_;
         st.jc = jc_;
         ApplyArgs &a = st.a;
         a.n = n_;
-        a.n_records = n_records;
+        a.n_records = (uint32_t)n_records;
         a.seed = p_.seed;
         a.first_sample = r.first_global;
-        a.lo = lo;
-        a.hi = std::min<uint32_t>(r.count, lo + kLargeBucket);
+        a.lo = a0;
+        a.hi = std::min<uint32_t>(hi, a0 + kLargeBucket);
         a.pass = r.pass;
         a.track_cross = r.track_cross ? 1 : 0;
         a.D = g_->diameter;
-        CK(cudaMemcpyAsync(d_state_, &st, sizeof(ApplyState), cudaMemcpyHostToDevice, stream));
-        CK(cudaGraphLaunch(apply_graph_, stream));
+        CK(cudaMemcpyAsync(d_state_, &st, sizeof(ApplyState), cudaMemcpyHostToDevice, stream_));
+        CK(cudaGraphLaunch(apply_graph_, stream_));
         launches += kApplyRoundKernels;
+        // the pinned argument ring is reused after kArgRing sub-rounds
+        if (arg_slot_ == 0) CK(cudaStreamSynchronize(stream_));
     }
     return SILVAN_OK;
 }
@@ -773,10 +795,12 @@ int Job::peel(double a, bool enabled) {
     CK(cudaMemcpy(d_lut_, lut.data(), sizeof(int32_t) * nbins, cudaMemcpyHostToDevice));
     CK(peel_map(jc_, n, d_lut_, idx_min, nbins, nullptr, stream_));
     launches += 1;
-    part_host_.resize(n);
-    CK(cudaMemcpyAsync(part_host_.data(), jc_.partition, sizeof(int32_t) * n,
-                       cudaMemcpyDeviceToHost, stream_));
-    CK(cudaStreamSynchronize(stream_));
+    if (!absolute_) {  // the top-k test looks partitions up per ranked node
+        part_host_.resize(n);
+        CK(cudaMemcpyAsync(part_host_.data(), jc_.partition, sizeof(int32_t) * n,
+                           cudaMemcpyDeviceToHost, stream_));
+        CK(cudaStreamSynchronize(stream_));
+    }
     return SILVAN_OK;
 }
 
@@ -938,7 +962,7 @@ int Job::stop_check(bool &stop) {
     out << "EVALUATING STOPPING CONDITION at iteration " << iteration_ << " (m=" << pass_samples_
         << ", d=" << dpb << ")" << "\n";
     const long long init = -(long long)pass_samples_;
-    CK(stop_reduce(jc_, n_, nparts_, init, d_red_, stream_));
+    CK(stop_reduce(jc_, nparts_, init, d_red_, stream_));
     launches += 2;
     CK(cudaMemcpyAsync(h_red_, d_red_, sizeof(StopReduction), cudaMemcpyDeviceToHost, stream_));
     JobScalars sc;
@@ -966,8 +990,14 @@ int Job::stop_check(bool &stop) {
     }
     eps_part_.assign(nparts_, 1.0);
     for (int i = 0; i < nparts_; i++) {
+        // nodes never updated in this pass hold mcrade = 0 in every trial
+        const bool zeros = R.touched[i] < part_count_[i];
         double avg = 0.0;
-        for (int j = 0; j < kTrials; j++) avg += R.mc_max[i * kTrials + j] / (double)kTrials;
+        for (int j = 0; j < kTrials; j++) {
+            const long long mj = zeros ? std::max(R.mc_max[i * kTrials + j], 0ll)
+                                       : R.mc_max[i * kTrials + j];
+            avg += mj / (double)kTrials;
+        }
         avg = avg / ms;
         const double sw = R.wimpy_max[i] / ms;
         const double dp = dpb / nparts_;
@@ -1044,7 +1074,7 @@ int Job::begin(FILE *sink, cudaStream_t stream) {
     CK(cudaEventRecord(ev_run_[0], stream_));
     phase_ = kPass1;
     alpha_ = p_.alpha;
-    global_next_ = 0;
+    base_global_ = 0;
     pass_samples_ = 0;
     // pass 1 stops after the first 11-sample block with n_pairs >= tau
     // (:828-845); top-k mode also needs 1.5 k nodes with approx >= 3
@@ -1056,13 +1086,25 @@ int Job::begin(FILE *sink, cudaStream_t stream) {
 bool Job::next_request(JobRequest &r) {
     if (phase_ == kDone || phase_ == kInit || error_) return false;
     uint64_t cnt = target_ - pass_samples_;
-    if (p_.form == SILVAN_FORM_PLAIN) cnt = std::min<uint64_t>(cnt, kBlock);
+    if (p_.form == SILVAN_FORM_PLAIN) {
+        cnt = std::min<uint64_t>(cnt, kBlock);
+    } else if (phase_ == kPass2) {
+        // draw ahead of the next schedule point: samples are deterministic in
+        // their index, so drawing early changes nothing but the launch count;
+        // the ones beyond the final stop are discarded
+        cnt = std::max<uint64_t>(cnt, lookahead_);
+        if (p_.m_hat) {
+            // the omega cap only decreases, so the run never goes beyond it
+            const uint64_t cap = (uint64_t)kBlock * (uint64_t)ceil(omega_ / kBlock);
+            if (cap > pass_samples_) cnt = std::min<uint64_t>(cnt, cap - pass_samples_);
+        }
+    }
     cnt = std::min<uint64_t>(cnt, kRoundSamples);
-    r.first_global = (uint32_t)global_next_;
+    r.first_global = (uint32_t)(base_global_ + pass_samples_);
     r.count = (uint32_t)cnt;
     r.pass = phase_ == kPass1 ? 1 : 2;
     r.track_cross = phase_ == kPass1 && !absolute_;
-    if (global_next_ + cnt >= 0xffffffffull) return false;
+    if (base_global_ + pass_samples_ + cnt >= 0xffffffffull) return false;
     return cnt > 0;
 }
 
@@ -1183,19 +1225,48 @@ int Job::finish_pass1() {
     flush();
     t2_start_ = now_seconds();
     phase_ = kPass2;
+    base_global_ = P1;
     pass_samples_ = 0;
     target_ = pass2_target(0, p_.m_hat != 0, omega_, next_stop_, last_stop_);
     return SILVAN_OK;
 }
 
-int Job::on_committed() {
-    // next_request is a pure function of the state, so the range the engine
-    // just committed is the one it returns now
-    JobRequest last;
-    if (!next_request(last)) return SILVAN_OK;
-    global_next_ += last.count;
-    pass_samples_ += last.count;
-    if (pass_samples_ < target_) return SILVAN_OK;
+int Job::on_drawn(const JobRequest &r, uint64_t n_records) {
+    // the drawn range is [lo, hi) in pass-local indices; commit it up to each
+    // schedule point in turn and evaluate the point (:828-845, :1060-1087)
+    const uint64_t lo = r.first_global - base_global_;
+    const uint64_t hi = lo + r.count;
+    if (lo != pass_samples_) {
+        set_error("drawn range does not continue the committed samples");
+        return SILVAN_E_STATE;
+    }
+    const uint64_t save_apply = launches;
+    CK(cudaEventRecord(ev_commit_[0], stream_));
+    for (;;) {
+        const uint64_t c_hi = std::min(target_, hi);
+        if (c_hi > pass_samples_) {
+            RK(apply_range(r, (uint32_t)(pass_samples_ - lo), (uint32_t)(c_hi - lo), n_records));
+            pass_samples_ = c_hi;
+        }
+        if (pass_samples_ < target_) break;  // the next point lies beyond the drawn range
+        const Phase ph = phase_;
+        RK(evaluate());
+        if (phase_ != ph || done()) break;    // new pass, or stopped
+        if (pass_samples_ != c_hi) break;     // pass 1 redrawn from the start
+    }
+    CK(cudaEventRecord(ev_commit_[1], stream_));
+    CK(cudaEventSynchronize(ev_commit_[1]));
+    if (launches != save_apply) {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, ev_commit_[0], ev_commit_[1]);
+        commit_ms_ += ms;
+    }
+    return SILVAN_OK;
+}
+
+// The reference's action at the end of the block where pass_samples_ reached
+// target_.
+int Job::evaluate() {
     if (phase_ == kPass1) {
         if (!absolute_ && !p1_final_) {
             // first block end with n_pairs >= tau and at least 1.5 k nodes
@@ -1234,7 +1305,6 @@ int Job::on_committed() {
                 CK(cudaMemsetAsync(jc_.cross_flag, 0, n, stream_));
                 CK(cudaMemsetAsync(jc_.sp_lengths, 0, sizeof(uint64_t) * (D + 1), stream_));
                 CK(cudaMemsetAsync(jc_.sc, 0, sizeof(JobScalars), stream_));
-                global_next_ = 0;
                 pass_samples_ = 0;
                 target_ = stop_at;
                 return SILVAN_OK;
@@ -1283,7 +1353,7 @@ int Job::on_committed() {
         << (double)sc2.void_samples / (double)N2 << ")" << "\n";
     const uint64_t vis_total = sc1_.vis_edges + sc2.vis_edges;
     const double t_bfs = own_engine_ ? own_engine_->sample_ms() / 1000.0 : 0.0;
-    const double t_crit = own_engine_ ? own_engine_->apply_ms() / 1000.0 : 0.0;
+    const double t_crit = commit_ms_ / 1000.0;
     if (p_.verbose > 0) {
         if (!absolute_) out << "eps_final_topk " << eps_final_topk_ << "\n";
         out << std::setprecision(6) << "\n" << "Finished after " << N2 << " iterations." << "\n";
@@ -1364,17 +1434,19 @@ int Job::run(silvan_result_t *res, FILE *sink) {
     RK(begin(sink, own_engine_->stream()));
     std::vector<Job *> jobs{this};
     std::vector<JobRequest> reqs(1);
+    std::vector<uint64_t> nrec;
     while (!done()) {
         if (!next_request(reqs[0])) {
             set_error("sample index space exhausted");
             return SILVAN_E_STATE;
         }
-        int rc = own_engine_->round(jobs, reqs, true, nullptr);
-        if (rc == SILVAN_OK) rc = on_committed();
+        int rc = own_engine_->round(jobs, reqs, nrec);
+        if (rc == SILVAN_OK) rc = on_drawn(reqs[0], nrec[0]);
         if (rc != SILVAN_OK) {
             error_ = rc;
             return rc;
         }
+        lookahead_ = own_engine_->free_samples();
     }
     return finish(res);
 }
@@ -1399,17 +1471,19 @@ int Job::step(uint32_t rounds, silvan_status_t *st, FILE *sink) {
     }
     std::vector<Job *> jobs{this};
     std::vector<JobRequest> reqs(1);
+    std::vector<uint64_t> nrec;
     for (uint32_t i = 0; i < rounds && !done(); i++) {
         if (!next_request(reqs[0])) {
             set_error("sample index space exhausted");
             return SILVAN_E_STATE;
         }
-        int rc = own_engine_->round(jobs, reqs, true, nullptr);
-        if (rc == SILVAN_OK) rc = on_committed();
+        int rc = own_engine_->round(jobs, reqs, nrec);
+        if (rc == SILVAN_OK) rc = on_drawn(reqs[0], nrec[0]);
         if (rc != SILVAN_OK) {
             error_ = rc;
             return rc;
         }
+        lookahead_ = own_engine_->free_samples();
     }
     if (st) {
         JobScalars sc{};
@@ -1464,8 +1538,11 @@ int run_batched(const std::vector<Job *> &jobs, uint64_t mem_budget, silvan_resu
             reqs.push_back(r);
         }
         if (act.empty()) break;
-        RK(eng.round(act, reqs, true, nullptr));
-        for (Job *j : act) RK(j->on_committed());
+        std::vector<uint64_t> nrec;
+        RK(eng.round(act, reqs, nrec));
+        for (size_t i = 0; i < act.size(); i++) RK(act[i]->on_drawn(reqs[i], nrec[i]));
+        const uint32_t la = eng.free_samples() / std::max<size_t>(1, act.size());
+        for (Job *j : act) j->set_lookahead(la);
     }
     for (size_t i = 0; i < jobs.size(); i++) RK(jobs[i]->finish(&results[i]));
     return SILVAN_OK;
@@ -1539,7 +1616,7 @@ int Job::replay(uint32_t first, uint32_t count, double alpha, std::vector<int32_
         reqs[0].first_global = first + done;
         reqs[0].count = c;
         reqs[0].pass = 1;
-        RK(own_engine_->round(jobs, reqs, false, &nrec));
+        RK(own_engine_->round(jobs, reqs, nrec));
         CK(cudaMemcpy(pl.data() + done, rb_.pl, sizeof(int32_t) * c, cudaMemcpyDeviceToHost));
         CK(cudaMemcpy(np.data() + done, rb_.np, sizeof(int32_t) * c, cudaMemcpyDeviceToHost));
         CK(cudaMemcpy(vis.data() + done, rb_.vis, sizeof(uint64_t) * c, cudaMemcpyDeviceToHost));

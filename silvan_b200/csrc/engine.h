@@ -99,12 +99,15 @@ class Engine {
     // With commit == false the round only draws (replay); `records` receives
     // the number of path-map records of each job.
     int round(const std::vector<Job *> &jobs, const std::vector<JobRequest> &reqs,
-              bool commit = true, std::vector<uint64_t> *records = nullptr);
+              std::vector<uint64_t> &records);
+    // samples that one more launch could draw for free: a launch lasts about
+    // as long as its slowest sample, during which the other slots keep
+    // drawing (0 until a launch has been measured)
+    uint32_t free_samples() const;
     uint64_t launches() const { return launches_; }
     float sample_ms() const { return sample_ms_; }
-    float apply_ms() const { return apply_ms_; }
     void reset_timers() {
-        sample_ms_ = apply_ms_ = 0;
+        sample_ms_ = 0;
         launches_ = 0;
     }
 
@@ -119,8 +122,11 @@ class Engine {
     cudaGraphExec_t sample_graph_ = nullptr;
     uint32_t graph_grid_ = 0;
     cudaEvent_t ev_[4] = {nullptr, nullptr, nullptr, nullptr};
-    float sample_ms_ = 0, apply_ms_ = 0;
+    float sample_ms_ = 0;
     uint64_t launches_ = 0;
+    double clock_khz_ = 0;
+    double cta_ms_per_sample_ = 0;
+    double last_launch_ms_ = 0;
 };
 
 class Job {
@@ -139,7 +145,10 @@ class Job {
     int begin(FILE *sink, cudaStream_t stream);
     bool done() const { return phase_ == kDone; }
     bool next_request(JobRequest &r);
-    int on_committed();  // after the last requested range was drawn and committed
+    // after the engine drew the requested range: commits it schedule point by
+    // schedule point and evaluates each point
+    int on_drawn(const JobRequest &r, uint64_t n_records);
+    void set_lookahead(uint32_t samples) { lookahead_ = samples; }
     int finish(silvan_result_t *res);
     int error() const { return error_; }
     uint32_t nodes() const { return n_; }
@@ -166,14 +175,14 @@ class Job {
     double alpha() const { return alpha_; }
     RoundBuffers &round_buffers() { return rb_; }
     int grow_records(uint64_t cap);
-    // commits the drawn range (records of the round already in rb_)
-    int apply(const JobRequest &r, uint32_t n_records, cudaStream_t stream);
     uint64_t launches = 0;
 
   private:
     enum Phase { kInit, kPass1, kPass2, kDone };
     int alloc_round(uint32_t max_samples, uint64_t rec_cap);
     int capture_apply(cudaStream_t stream);
+    int apply_range(const JobRequest &r, uint32_t lo, uint32_t hi, uint64_t n_records);
+    int evaluate();
     int sync_scalars(JobScalars &sc);
     int read_sp_lengths(std::vector<uint64_t> &out);
     int peel(double a, bool enabled);
@@ -214,7 +223,10 @@ class Job {
     bool peel_on_ = true;
     double peel_a_ = 2.0;
     uint32_t k_ = 0, union_sample_ = 0, tau_ = 0;
-    uint64_t global_next_ = 0;   // global index of the next sample to draw
+    uint64_t base_global_ = 0;   // global index of the pass's first sample
+    uint32_t lookahead_ = 0;     // pass 2: samples drawn ahead of the next point
+    float commit_ms_ = 0;
+    cudaEvent_t ev_commit_[2] = {nullptr, nullptr};
     uint64_t pass_samples_ = 0;  // samples committed in the current pass
     uint64_t target_ = 0;        // sample count of the next schedule event
     uint64_t p1_chunk_ = 0;      // top-k pass 1: speculative chunk size

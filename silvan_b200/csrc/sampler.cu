@@ -12,15 +12,16 @@
 // predecessor lists are appended in scan order, and meeting edges are
 // collected in scan order.  Here the items of a level are numbered
 // g = 0, 1, ... in exactly that order and processed in tiles of ascending g:
-//   phase 1  every item reads the state of its neighbour y; an unvisited y is
-//            claimed with a CAS, and every item that reaches a node of the new
-//            level records itself with atomicMin/atomicMax of (g << 32 | x)
-//            (the first and the last predecessor), a count and sigma += sigma(x)
-//            (a wrapping sum, order-free);
+//   phase 1  every item reads the state of its neighbour y; every item that
+//            reaches a node of the new level (unvisited, or joined earlier in
+//            this level) records itself with atomicMin/atomicMax of
+//            (g << 32 | x) (the first and the last predecessor), a count and
+//            sigma += sigma(x) (a wrapping sum, order-free);
 //   phase 2  after a barrier the items whose g equals their node's minimum are
-//            the joining hits; they and the meeting items are compacted in g
-//            order (warp ballots plus one block scan), which appends new nodes
-//            to the queue and meeting edges to the list in the reference order.
+//            the joining hits; they mark their node as visited and, with the
+//            meeting items, are compacted in g order (warp ballots plus one
+//            block scan), which appends new nodes to the queue and meeting
+//            edges to the list in the reference order.
 // A later tile can never lower a node's minimum below an earlier tile's g, so
 // each tile is final once its own phase 1 is done.
 //
@@ -271,11 +272,10 @@ __device__ void expand_level(const SegDesc &A, SamplerSmem &s, NodeRec *rec,
                     const uint32_t y = adj[s.f_off[l] + (it - s.f_pre[l])];
                     xs[k] = x;
                     ys[k] = y;
-                    uint32_t sty = __ldcg(&rec[y].st);
-                    if (sty == 0u) {
-                        atomicCAS(&rec[y].st, 0u, new_st);
-                        code[k] = 1;
-                    } else if (sty == new_st) {
+                    // unvisited, or joined earlier in this level: a new-level
+                    // hit (the joining hit marks the node in phase 2)
+                    const uint32_t sty = __ldcg(&rec[y].st);
+                    if (sty == 0u || sty == new_st) {
                         code[k] = 1;
                     } else if (st_side(sty) != side) {
                         code[k] = 2;
@@ -344,6 +344,7 @@ __device__ void expand_level(const SegDesc &A, SamplerSmem &s, NodeRec *rec,
                 if (code[k] == 1) {
                     const uint32_t y = ys[k];
                     queue[nb + rn[k]] = y;
+                    rec[y].st = new_st;
                     sum_local += off[y + 1] - off[y];
                 } else if (code[k] == 2) {
                     uint32_t pos = mb + rm[k];
@@ -416,6 +417,7 @@ __global__ void __launch_bounds__(kSamplerBlock, 2) sampler_kernel(SamplerLaunch
         __syncthreads();
         const uint32_t sl = s.work - A.base;
         const uint32_t gidx = A.first_sample + sl;
+        const long long t_sample0 = clock64();
 
         // ---- endpoints (Sp_sampler.cpp:46,58-60) and void test (:62-74) -------
         if (threadIdx.x == 0) {
@@ -444,6 +446,7 @@ __global__ void __launch_bounds__(kSamplerBlock, 2) sampler_kernel(SamplerLaunch
                 A.out_status[sl] = 0;
                 A.out_ball[sl] = 0;
                 A.out_pred[sl] = 0;
+                atomicAdd(&L.hdr->cycles, (unsigned long long)(clock64() - t_sample0));
             }
             __syncthreads();
             continue;
@@ -664,6 +667,7 @@ __global__ void __launch_bounds__(kSamplerBlock, 2) sampler_kernel(SamplerLaunch
             A.out_status[sl] = s.status;
             A.out_ball[sl] = s.end_q;
             A.out_pred[sl] = s.pred_hits;
+            atomicAdd(&L.hdr->cycles, (unsigned long long)(clock64() - t_sample0));
         }
         __syncthreads();
     }
@@ -672,7 +676,10 @@ __global__ void __launch_bounds__(kSamplerBlock, 2) sampler_kernel(SamplerLaunch
 __global__ void round_begin_kernel(SamplerLaunch L, uint32_t max_segs) {
     const uint32_t ns = min(L.hdr->nsegs, max_segs);
     for (uint32_t i = threadIdx.x; i < ns; i += blockDim.x) *L.segs[i].rec_cursor = 0ull;
-    if (threadIdx.x == 0) L.hdr->work = 0;
+    if (threadIdx.x == 0) {
+        L.hdr->work = 0;
+        L.hdr->cycles = 0;
+    }
 }
 
 __global__ void init_slots_kernel(NodeRec *rec, uint32_t *hits, uint64_t total) {

@@ -49,6 +49,7 @@ struct RoundHeader {
     uint32_t total;   // samples over all segments
     uint32_t work;    // next work index (zeroed by round_begin)
     uint32_t pad;
+    unsigned long long cycles;  // SM cycles spent in samples (zeroed by round_begin)
 };
 
 struct SlotArrays {

@@ -132,15 +132,19 @@ struct Server {
                 samples += q.count;
             }
             if (jobs.empty()) continue;
-            int rc = eng.round(jobs, reqs, true, nullptr);
+            std::vector<uint64_t> nrec;
+            int rc = eng.round(jobs, reqs, nrec);
             rounds++;
             if (rc != SILVAN_OK) {
                 // a device error poisons every job in the round
                 for (ServerRequest *r : owners) finish(r, rc);
                 continue;
             }
-            for (ServerRequest *r : owners) {
-                int e = r->job->on_committed();
+            const uint32_t la = eng.free_samples() / std::max<size_t>(1, owners.size());
+            for (size_t i = 0; i < owners.size(); i++) {
+                ServerRequest *r = owners[i];
+                int e = r->job->on_drawn(reqs[i], nrec[i]);
+                r->job->set_lookahead(la);
                 if (e != SILVAN_OK) finish(r, e);
                 else if (r->job->done()) finish(r, SILVAN_OK);
             }
