@@ -198,6 +198,8 @@ def main():
     ap.add_argument("--slots", type=int, default=0,
                     help="sampler slots (0 = occupancy x SMs); small values bound the device "
                          "memory for profiler captures")
+    ap.add_argument("--block", type=int, default=0, choices=[0, 128, 256, 512, 1024],
+                    help="threads per sampler slot (0 = autotuned per graph and round)")
     args = ap.parse_args()
     cfg = CONFIGS[args.config]
     if args.impl == "reference":
@@ -223,7 +225,7 @@ def main():
 
     def one_run(seed):
         job = sb.Probabilistic(g, cfg["eps"], cfg["delta"], k=cfg["k"], seed=seed,
-                               form=args.form, slots=args.slots)
+                               form=args.form, slots=args.slots, block=args.block)
         res = job.run()
         del job
         return res
@@ -271,7 +273,8 @@ def main():
         t0 = time.perf_counter()
         g2 = sb.Graph.upload(pcsr, with_cc=True)
         job = sb.Probabilistic(g2, cfg["eps"], cfg["delta"], k=cfg["k"],
-                               seed=seed0 + 50 + s, form=args.form, slots=args.slots)
+                               seed=seed0 + 50 + s, form=args.form, slots=args.slots,
+                               block=args.block)
         r = job.run()
         job.get_centrality(out=est_t.numpy())
         torch.cuda.synchronize()
@@ -326,7 +329,10 @@ def main():
             "config": {"workload": cfg["workload"], "n": csr.n, "m": int(csr.out_off[-1]),
                        "eps": cfg["eps"], "delta": cfg["delta"], "form": args.form,
                        "parallelism": "replicas" if world > 1 else "single",
-                       "l2": "working set above L2 (CSR 128 MB + per-slot state)"},
+                       "l2": "working set above L2 (CSR 128 MB + per-slot state)",
+                       "sampler_block": [r["sampler_block"] for r in results],
+                       "sampler_launches_per_step": sum(r["sampler_launches"] for r in results)
+                       / args.steps},
             "time_to_guarantee_ms": 1000 * t_max / args.steps,
             "samples_per_step": samples_all / max(1, world) / args.steps,
             "backtracked_paths_per_step": sum(r["backtracked_paths"] for r in results) /

@@ -76,7 +76,8 @@ typedef struct {
     uint32_t np_cap;     /* max paths per sample (0 = default 2^24)         */
     uint32_t slots;      /* concurrent sampler slots (0 = autotuned)        */
     uint32_t threads;    /* divisor of union_sample (0 = 1, parity mode)    */
-    uint32_t reserved;
+    uint32_t block;      /* threads per sampler slot: 0 = autotuned per graph
+                            and round, else 128, 256, 512 or 1024            */
 } silvan_params_t;
 
 /* Fills p with the reference defaults. */
@@ -114,6 +115,8 @@ typedef struct {
     uint64_t ball_nodes;         /* nodes visited by all samples            */
     uint64_t pred_entries;       /* predecessor entries of all samples      */
     uint64_t kernel_launches;    /* kernels launched by the run             */
+    uint32_t sampler_launches;   /* persistent sampler launches (own engine) */
+    uint32_t sampler_block;      /* CTA size that drew most samples          */
 } silvan_result_t;
 
 /* ---- graphs (reference: Graph, silvan/src/Graph.cpp) ------------------- */

@@ -58,7 +58,7 @@ class Params(C.Structure):
                 ("m_hat", C.c_int32), ("alpha", C.c_double), ("alpha_given", C.c_int32),
                 ("form", C.c_int32), ("a", C.c_double), ("seed", C.c_uint64),
                 ("verbose", C.c_double), ("np_cap", C.c_uint32), ("slots", C.c_uint32),
-                ("threads", C.c_uint32), ("reserved", C.c_uint32)]
+                ("threads", C.c_uint32), ("block", C.c_uint32)]
 
 
 class Result(C.Structure):
@@ -76,7 +76,8 @@ class Result(C.Structure):
                 ("time_total_s", C.c_double), ("time_first_pass_s", C.c_double),
                 ("time_sampling_s", C.c_double), ("time_apply_s", C.c_double),
                 ("time_device_s", C.c_double), ("ball_nodes", C.c_uint64),
-                ("pred_entries", C.c_uint64), ("kernel_launches", C.c_uint64)]
+                ("pred_entries", C.c_uint64), ("kernel_launches", C.c_uint64),
+                ("sampler_launches", C.c_uint32), ("sampler_block", C.c_uint32)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}
@@ -362,7 +363,7 @@ class Probabilistic:
 
     def __init__(self, graph: Graph, eps, delta, k=0, alpha=2.3, alpha_given=False, a=2.0,
                  m_hat=True, seed=42, form="batched", verbose=0.0, np_cap=0, slots=0,
-                 threads=1):
+                 threads=1, block=0):
         lib = load()
         p = Params()
         lib.silvan_params_default(C.byref(p))
@@ -370,7 +371,7 @@ class Probabilistic:
         p.alpha, p.alpha_given, p.a = alpha, int(alpha_given), a
         p.m_hat, p.seed, p.verbose = int(m_hat), seed, verbose
         p.form = FORM_PLAIN if form == "plain" else FORM_BATCHED
-        p.np_cap, p.slots, p.threads = np_cap, slots, threads
+        p.np_cap, p.slots, p.threads, p.block = np_cap, slots, threads, block
         self.graph = graph
         self.params = p
         h = C.c_void_p()

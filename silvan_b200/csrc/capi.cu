@@ -87,6 +87,7 @@ void silvan_params_default(silvan_params_t *p) {
     p->np_cap = 0;
     p->slots = 0;
     p->threads = 1;
+    p->block = 0;
 }
 
 const char *silvan_last_error(void) { return last_error_cstr(); }

@@ -2,6 +2,7 @@
 #include "engine.h"
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstring>
@@ -238,7 +239,7 @@ void SlotPool::free_all() {
 // ---------------------------------------------------------------------------
 Engine::~Engine() {
     if (stream_) cudaStreamSynchronize(stream_);
-    if (sample_graph_) cudaGraphExecDestroy(sample_graph_);
+    drop_execs();
     dfree(d_hdr_);
     dfree(d_segs_);
     dfree(d_cursors_);
@@ -260,12 +261,19 @@ int Engine::init(uint64_t n_max, uint32_t slots, uint64_t mem_budget) {
         clock_khz_ = khz;
     }
     for (auto &e : ev_) CK(cudaEventCreate(&e));
-    if (slots == 0) {
-        int dev = 0, sms = 0;
+    int sms = 0;
+    {
+        int dev = 0;
         CK(cudaGetDevice(&dev));
         CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-        slots = (uint32_t)(sms * std::max(1, sampler_max_ctas_per_sm()));
     }
+    uint32_t resident[kNB];
+    uint32_t most = 0;
+    for (int b = 0; b < kNB; b++) {
+        resident[b] = (uint32_t)sms * (uint32_t)std::max(0, sampler_max_ctas_per_sm(kSamplerBlocks[b]));
+        most = std::max(most, resident[b]);
+    }
+    if (slots == 0) slots = std::max<uint32_t>(most, 1);
     if (mem_budget == 0) {
         size_t fr = 0, tot = 0;
         CK(cudaMemGetInfo(&fr, &tot));
@@ -274,6 +282,7 @@ int Engine::init(uint64_t n_max, uint32_t slots, uint64_t mem_budget) {
     const uint64_t fit = mem_budget / std::max<uint64_t>(SlotPool::bytes_per_slot(n_max), 1);
     if (fit < slots) slots = (uint32_t)std::max<uint64_t>(fit, 1);
     RK(slots_.alloc(slots, n_max, stream_));
+    for (int b = 0; b < kNB; b++) max_grid_[b] = std::min(resident[b], slots);
     RK(dmalloc(&d_hdr_, 1));
     RK(hmalloc(&h_hdr_, 1));
     return ensure_segs(64);
@@ -292,9 +301,94 @@ int Engine::ensure_segs(uint32_t nsegs) {
     RK(hmalloc(&h_segs_, cap));
     RK(hmalloc(&h_cursors_, cap));
     max_segs_ = cap;
-    if (sample_graph_) cudaGraphExecDestroy(sample_graph_);
-    sample_graph_ = nullptr;
+    drop_execs();
     return SILVAN_OK;
+}
+
+void Engine::drop_execs() {
+    for (Exec &x : execs_) cudaGraphExecDestroy(x.exec);
+    execs_.clear();
+}
+
+// The round's two kernels (round_begin + sampler) captured once per (CTA
+// size, grid) and replayed with new segments.
+int Engine::sampler_exec(int block, uint32_t grid, cudaGraphExec_t *out) {
+    for (const Exec &x : execs_)
+        if (x.block == block && x.grid == grid) {
+            *out = x.exec;
+            return SILVAN_OK;
+        }
+    SamplerLaunch L{};
+    L.slots = SlotArrays{slots_.rec,  slots_.queue,    slots_.hits, slots_.touched,
+                         slots_.meet, slots_.meet_pre, slots_.n};
+    L.hdr = d_hdr_;
+    L.segs = d_segs_;
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+    cudaError_t e1 = sampler_round_begin(L, max_segs_, stream_);
+    cudaError_t e2 = sampler_launch(L, grid, stream_, block);
+    cudaError_t e3 = cudaStreamEndCapture(stream_, &g);
+    CK(e1);
+    CK(e2);
+    CK(e3);
+    cudaGraphExec_t x = nullptr;
+    cudaError_t e4 = cudaGraphInstantiate(&x, g, 0);
+    cudaGraphDestroy(g);
+    CK(e4);
+    if (execs_.size() >= 16) drop_execs();
+    execs_.push_back(Exec{block, grid, x});
+    *out = x;
+    return SILVAN_OK;
+}
+
+// Autotuned CTA size of a round.  Every CTA size is tried once on each graph
+// (the samples are the same whichever size draws them); after that the round
+// takes the size with the least predicted time: the slowest sample of the
+// round, or the CTA time of all its samples spread over the resident CTAs,
+// whichever is longer.
+int Engine::choose_block(const std::vector<Job *> &jobs, const std::vector<JobRequest> &reqs,
+                         const std::vector<uint32_t> &idx, uint32_t total) const {
+    const silvan_params_t &p0 = jobs[idx[0]]->params();
+    if (p0.block) return (int)p0.block;
+    if (p0.form == SILVAN_FORM_PLAIN) return kSamplerBlock;
+    static const int order[kNB] = {2, 1, 0, 3};  // 512, 256, 128, 1024
+    for (int oi = 0; oi < kNB; oi++) {
+        const int b = order[oi];
+        if (!max_grid_[b]) continue;
+        for (uint32_t i : idx) {
+            auto it = stats_.find(jobs[i]->graph()->uid);
+            if (it == stats_.end() || it->second[b].rounds == 0) return kSamplerBlocks[b];
+        }
+    }
+    int best = kSamplerBlock;
+    double best_t = 1e300;
+    for (int b = 0; b < kNB; b++) {
+        if (!max_grid_[b]) continue;
+        double tail = 0, work = 0;
+        for (uint32_t i : idx) {
+            const BlockStats &st = stats_.at(jobs[i]->graph()->uid)[b];
+            tail = std::max(tail, st.tail_ms);
+            work += reqs[i].count * st.cta_ms;
+        }
+        const double t = std::max(tail, work / std::min(max_grid_[b], total));
+        if (t < best_t) {
+            best_t = t;
+            best = kSamplerBlocks[b];
+        }
+    }
+    return best;
+}
+
+uint32_t Engine::main_block() const {
+    int b = 2;
+    for (int i = 0; i < kNB; i++)
+        if (block_samples_[i] > block_samples_[b]) b = i;
+    return (uint32_t)kSamplerBlocks[b];
+}
+
+uint64_t DeviceGraph::next_uid() {
+    static std::atomic<uint64_t> c{1};
+    return c.fetch_add(1);
 }
 
 int Engine::round(const std::vector<Job *> &jobs, const std::vector<JobRequest> &reqs,
@@ -348,36 +442,27 @@ int Engine::round(const std::vector<Job *> &jobs, const std::vector<JobRequest> 
     h_hdr_->total = total;
     h_hdr_->work = 0;
     h_hdr_->cycles = 0;
-    const uint32_t grid = std::min<uint32_t>(slots_.slots, total);
+    h_hdr_->max_cycles = 0;
+    const int block = choose_block(jobs, reqs, idx, total);
+    int bi = -1;
+    for (int b = 0; b < kNB; b++)
+        if (kSamplerBlocks[b] == block && max_grid_[b]) bi = b;
+    if (bi < 0) {
+        set_error("sampler CTA size must be 128, 256, 512 or 1024 threads");
+        return SILVAN_E_BADARG;
+    }
+    const uint32_t grid = std::min<uint32_t>(max_grid_[bi], total);
+    cudaGraphExec_t exec = nullptr;
+    RK(sampler_exec(block, grid, &exec));
     for (;;) {
         CK(cudaMemcpyAsync(d_segs_, h_segs_, sizeof(SegDesc) * idx.size(),
                            cudaMemcpyHostToDevice, stream_));
         CK(cudaMemcpyAsync(d_hdr_, h_hdr_, sizeof(RoundHeader), cudaMemcpyHostToDevice, stream_));
-        if (!sample_graph_ || graph_grid_ != grid) {
-            if (sample_graph_) cudaGraphExecDestroy(sample_graph_);
-            sample_graph_ = nullptr;
-            SamplerLaunch L{};
-            L.slots = SlotArrays{slots_.rec,  slots_.queue, slots_.hits,    slots_.touched,
-                                 slots_.meet, slots_.meet_pre, slots_.n};
-            L.hdr = d_hdr_;
-            L.segs = d_segs_;
-            cudaGraph_t g = nullptr;
-            CK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
-            cudaError_t e1 = sampler_round_begin(L, max_segs_, stream_);
-            cudaError_t e2 = sampler_launch(L, grid, stream_);
-            cudaError_t e3 = cudaStreamEndCapture(stream_, &g);
-            CK(e1);
-            CK(e2);
-            CK(e3);
-            cudaError_t e4 = cudaGraphInstantiate(&sample_graph_, g, 0);
-            cudaGraphDestroy(g);
-            CK(e4);
-            graph_grid_ = grid;
-        }
         CK(cudaEventRecord(ev_[0], stream_));
-        CK(cudaGraphLaunch(sample_graph_, stream_));
+        CK(cudaGraphLaunch(exec, stream_));
         CK(cudaEventRecord(ev_[1], stream_));
         launches_ += 2;
+        sampler_launches_++;
         CK(cudaMemcpyAsync(h_cursors_, d_cursors_, sizeof(unsigned long long) * idx.size(),
                            cudaMemcpyDeviceToHost, stream_));
         CK(cudaMemcpyAsync(h_hdr_, d_hdr_, sizeof(RoundHeader), cudaMemcpyDeviceToHost, stream_));
@@ -385,13 +470,22 @@ int Engine::round(const std::vector<Job *> &jobs, const std::vector<JobRequest> 
         float ms = 0;
         cudaEventElapsedTime(&ms, ev_[0], ev_[1]);
         sample_ms_ += ms;
-        // cost model for speculative draws: a launch lasts about as long as
-        // its slowest sample, so the samples that fit into that time on the
-        // other slots cost (almost) nothing extra
+        block_samples_[bi] += total;
+        // cost model of the CTA-size choice and of speculative draws: a launch
+        // lasts about as long as its slowest sample, so the samples that fit
+        // into that time on the other slots cost (almost) nothing extra
         if (h_hdr_->total > 0 && clock_khz_ > 0) {
             const double cta_ms = (double)h_hdr_->cycles / clock_khz_ / h_hdr_->total;
-            cta_ms_per_sample_ = cta_ms_per_sample_ > 0 ? 0.5 * (cta_ms_per_sample_ + cta_ms) : cta_ms;
+            const double tail_ms = (double)h_hdr_->max_cycles / clock_khz_;
+            last_cta_ms_ = cta_ms;
             last_launch_ms_ = ms;
+            last_grid_ = grid;
+            for (uint32_t i : idx) {
+                BlockStats &st = stats_[jobs[i]->graph()->uid][bi];
+                st.cta_ms = st.rounds ? 0.5 * (st.cta_ms + cta_ms) : cta_ms;
+                st.tail_ms = st.rounds ? 0.5 * (st.tail_ms + tail_ms) : tail_ms;
+                st.rounds++;
+            }
         }
         bool redo = false;
         uint32_t base = 0;
@@ -412,14 +506,15 @@ int Engine::round(const std::vector<Job *> &jobs, const std::vector<JobRequest> 
         h_hdr_->total = total;
         h_hdr_->work = 0;
         h_hdr_->cycles = 0;
+        h_hdr_->max_cycles = 0;
     }
     for (uint32_t s = 0; s < idx.size(); s++) records[idx[s]] = h_cursors_[s];
     return SILVAN_OK;
 }
 
 uint32_t Engine::free_samples() const {
-    if (cta_ms_per_sample_ <= 0 || last_launch_ms_ <= 0) return 0;
-    const double f = last_launch_ms_ * slots_.slots / cta_ms_per_sample_;
+    if (last_cta_ms_ <= 0 || last_launch_ms_ <= 0) return 0;
+    const double f = last_launch_ms_ * last_grid_ / last_cta_ms_;
     return (uint32_t)std::min<double>(f, (double)kRoundSamples);
 }
 
@@ -603,6 +698,11 @@ int Job::init() {
     n_ = g_->n;
     if (!(p_.eps > 0 && p_.eps < 1) || !(p_.delta > 0 && p_.delta < 1)) {
         set_error("eps and delta must lie in (0, 1)");
+        return SILVAN_E_BADARG;
+    }
+    if (p_.block != 0 && p_.block != 128 && p_.block != 256 && p_.block != 512 &&
+        p_.block != 1024) {
+        set_error("block must be 0 (autotuned), 128, 256, 512 or 1024");
         return SILVAN_E_BADARG;
     }
     if (p_.np_cap == 0) p_.np_cap = 1u << 24;
@@ -1410,6 +1510,8 @@ int Job::evaluate() {
     res.ball_nodes = sc1_.ball_nodes + sc2.ball_nodes;
     res.pred_entries = sc1_.pred_entries + sc2.pred_entries;
     res.kernel_launches = launches + (own_engine_ ? own_engine_->launches() : 0);
+    res.sampler_launches = own_engine_ ? own_engine_->sampler_launches() : 0;
+    res.sampler_block = own_engine_ ? own_engine_->main_block() : 0;
     phase_ = kDone;
     return SILVAN_OK;
 }

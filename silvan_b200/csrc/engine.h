@@ -5,12 +5,14 @@
 // work is the concatenation of every job's request).  A Job owns its counters
 // and round buffers and restates Probabilistic::run
 // (silvan/src/Probabilistic.cpp:775-1139) as a state machine: it asks for the
-// next range of samples, and after the engine has drawn and committed them it
-// evaluates the schedule events the reference evaluates at that point.
+// next range of samples, and after the engine has drawn them it commits them
+// and evaluates the schedule events the reference evaluates at each point.
 #pragma once
+#include <array>
 #include <cstdint>
 #include <cstdio>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -44,6 +46,8 @@ struct DeviceGraph {
     uint32_t *d_in_off = nullptr, *d_in_adj = nullptr;
     uint32_t *d_cc = nullptr;
     int device = 0;
+    uint64_t uid = next_uid();  // keys the sampler's per-graph schedule statistics
+    static uint64_t next_uid();
 
     int upload();  // from `host` and `cc`
     // from caller-owned host arrays (ideally pinned): copied straight to the
@@ -93,11 +97,10 @@ class Engine {
     uint64_t n_max() const { return slots_.n; }
     uint32_t slots() const { return slots_.slots; }
     cudaStream_t stream() const { return stream_; }
-    // Draws every job's requested range in one persistent launch, then
-    // commits each range to its job (ordered apply).  Grows a job's record
-    // buffer and redraws the round when the path maps did not fit.
-    // With commit == false the round only draws (replay); `records` receives
-    // the number of path-map records of each job.
+    // Draws every job's requested range in one persistent launch into the
+    // jobs' round buffers; the jobs commit them.  Grows a job's record buffer
+    // and redraws the round when the path maps did not fit.  `records`
+    // receives the number of path-map records of each job.
     int round(const std::vector<Job *> &jobs, const std::vector<JobRequest> &reqs,
               std::vector<uint64_t> &records);
     // samples that one more launch could draw for free: a launch lasts about
@@ -109,24 +112,49 @@ class Engine {
     void reset_timers() {
         sample_ms_ = 0;
         launches_ = 0;
+        sampler_launches_ = 0;
+        block_samples_.fill(0);
     }
+    uint32_t sampler_launches() const { return sampler_launches_; }
+    // CTA size that drew the most samples since reset_timers()
+    uint32_t main_block() const;
 
   private:
+    static constexpr int kNB = 4;  // compiled CTA sizes (kSamplerBlocks)
+    // Measured cost of one graph's samples under each CTA size: CTA time
+    // per sample (throughput) and the slowest sample of a round (its tail).
+    struct BlockStats {
+        double cta_ms = 0, tail_ms = 0;
+        uint32_t rounds = 0;
+    };
+    struct Exec {
+        int block;
+        uint32_t grid;
+        cudaGraphExec_t exec;
+    };
     int ensure_segs(uint32_t nsegs);
+    int choose_block(const std::vector<Job *> &jobs, const std::vector<JobRequest> &reqs,
+                     const std::vector<uint32_t> &idx, uint32_t total) const;
+    int sampler_exec(int block, uint32_t grid, cudaGraphExec_t *out);
+    void drop_execs();
     SlotPool slots_;
     cudaStream_t stream_ = nullptr;
     RoundHeader *d_hdr_ = nullptr, *h_hdr_ = nullptr;
     SegDesc *d_segs_ = nullptr, *h_segs_ = nullptr;
     unsigned long long *d_cursors_ = nullptr, *h_cursors_ = nullptr;
     uint32_t max_segs_ = 0;
-    cudaGraphExec_t sample_graph_ = nullptr;
-    uint32_t graph_grid_ = 0;
+    std::vector<Exec> execs_;          // captured round_begin + sampler per (block, grid)
+    uint32_t max_grid_[kNB] = {};      // resident CTAs per CTA size (0 = unusable)
+    std::unordered_map<uint64_t, std::array<BlockStats, kNB>> stats_;  // by graph uid
+    std::array<uint64_t, kNB> block_samples_{};
+    uint32_t sampler_launches_ = 0;
     cudaEvent_t ev_[4] = {nullptr, nullptr, nullptr, nullptr};
     float sample_ms_ = 0;
     uint64_t launches_ = 0;
     double clock_khz_ = 0;
-    double cta_ms_per_sample_ = 0;
+    double last_cta_ms_ = 0;     // CTA ms per sample of the last launch
     double last_launch_ms_ = 0;
+    uint32_t last_grid_ = 0;
 };
 
 class Job {

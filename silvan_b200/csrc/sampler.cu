@@ -36,13 +36,25 @@ namespace silvan {
 
 namespace {
 
-constexpr int kWarps = kSamplerBlock / 32;
-constexpr int kItems = 4;                      // scan items per lane per tile
-constexpr int kTile = kSamplerBlock * kItems;  // scan items per tile
-constexpr int kChunk = 2048;                   // frontier nodes staged at once
-constexpr int kMaxLevels = 256;                // levels per side with recorded bounds
+constexpr int kItems = 4;        // scan items per lane per tile
+constexpr int kMaxLevels = 256;  // levels per side with recorded bounds
 
+// Per-CTA-size constants: BLOCK threads serve one sample.  Smaller CTAs put
+// more samples in flight per SM (throughput on many short searches), larger
+// ones put more threads on one wide level (the slowest sample of a round).
+template <int BLOCK>
+struct Shape {
+    static constexpr int kWarps = BLOCK / 32;
+    static constexpr int kTile = BLOCK * kItems;                    // scan items per tile
+    static constexpr int kChunk = BLOCK * 4 < 2048 ? BLOCK * 4 : 2048;  // frontier nodes staged
+    static constexpr int kPerThread = kChunk / BLOCK;
+    static constexpr int kMinBlocks = 1024 / BLOCK;                 // 64 registers per thread
+};
+
+template <int BLOCK>
 struct SamplerSmem {
+    static constexpr int kWarps = Shape<BLOCK>::kWarps;
+    static constexpr int kChunk = Shape<BLOCK>::kChunk;
     uint32_t f_node[kChunk];
     uint32_t f_off[kChunk];
     uint32_t f_pre[kChunk + 1];
@@ -85,7 +97,9 @@ __device__ __forceinline__ uint32_t draw32(uint64_t seed, uint32_t sample, uint3
 
 // Exclusive block scan of one value per thread; returns the block total.
 // tmp needs kWarps + 1 entries.
+template <int BLOCK>
 __device__ uint32_t block_exclusive_scan(uint32_t v, uint32_t &excl, uint32_t *tmp) {
+    constexpr int kWarps = Shape<BLOCK>::kWarps;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     uint32_t incl = v;
 #pragma unroll
@@ -126,7 +140,8 @@ __device__ __forceinline__ void rec_reset(NodeRec *r) {
 //   level scan: walk the level's queue segment, binary-search a in each row;
 //   reverse scan: walk a's reverse row, keep the candidates on level d-1 and
 //                 rank them by their own queue position (their first hit).
-__device__ uint32_t middle_pred(const SegDesc &A, const SamplerSmem &s, const NodeRec *rec,
+template <class Smem>
+__device__ uint32_t middle_pred(const SegDesc &A, const Smem &s, const NodeRec *rec,
                                 const uint32_t *queue, uint32_t a, uint32_t st_a, uint32_t t,
                                 int32_t &status) {
     const uint32_t side = st_side(st_a);
@@ -202,7 +217,8 @@ __device__ uint32_t middle_pred(const SegDesc &A, const SamplerSmem &s, const No
     return bx;
 }
 
-__device__ __forceinline__ void note_hit(uint32_t *hits, uint32_t *touched, SamplerSmem &s,
+template <class Smem>
+__device__ __forceinline__ void note_hit(uint32_t *hits, uint32_t *touched, Smem &s,
                                          uint32_t a) {
     if (atomicAdd(&hits[a], 1u) == 0u) {
         uint32_t i = atomicAdd(&s.ntouched, 1u);
@@ -211,9 +227,14 @@ __device__ __forceinline__ void note_hit(uint32_t *hits, uint32_t *touched, Samp
 }
 
 // Expands one BFS level of `side` (silvan/src/Sp_sampler.cpp:89-143).
-__device__ void expand_level(const SegDesc &A, SamplerSmem &s, NodeRec *rec,
+template <int BLOCK>
+__device__ void expand_level(const SegDesc &A, SamplerSmem<BLOCK> &s, NodeRec *rec,
                              uint32_t *queue, uint2 *meet, uint32_t side, uint32_t lo,
                              uint32_t hi, uint32_t depth) {
+    constexpr int kWarps = Shape<BLOCK>::kWarps;
+    constexpr int kTile = Shape<BLOCK>::kTile;
+    constexpr int kChunk = Shape<BLOCK>::kChunk;
+    constexpr int kPer = Shape<BLOCK>::kPerThread;
     const uint32_t *off = side == kSideU ? A.out_off : A.in_off;
     const uint32_t *adj = side == kSideU ? A.out_adj : A.in_adj;
     const uint32_t new_st = st_make(side, depth + 1u);
@@ -224,11 +245,11 @@ __device__ void expand_level(const SegDesc &A, SamplerSmem &s, NodeRec *rec,
     for (uint32_t c0 = lo; c0 < hi; c0 += kChunk) {
         const uint32_t nc = min((uint32_t)kChunk, hi - c0);
         // stage the chunk: row starts, degrees (prefix), sigma
-        uint32_t degs[kChunk / kSamplerBlock];
+        uint32_t degs[kPer];
         uint32_t tsum = 0;
 #pragma unroll
-        for (int i = 0; i < kChunk / kSamplerBlock; i++) {
-            uint32_t p = threadIdx.x * (kChunk / kSamplerBlock) + i;
+        for (int i = 0; i < kPer; i++) {
+            uint32_t p = threadIdx.x * kPer + i;
             uint32_t d = 0;
             if (p < nc) {
                 uint32_t x = __ldcg(&queue[c0 + p]);
@@ -242,10 +263,10 @@ __device__ void expand_level(const SegDesc &A, SamplerSmem &s, NodeRec *rec,
             tsum += d;
         }
         uint32_t excl;
-        uint32_t total = block_exclusive_scan(tsum, excl, s.scan_tmp);
+        uint32_t total = block_exclusive_scan<BLOCK>(tsum, excl, s.scan_tmp);
 #pragma unroll
-        for (int i = 0; i < kChunk / kSamplerBlock; i++) {
-            uint32_t p = threadIdx.x * (kChunk / kSamplerBlock) + i;
+        for (int i = 0; i < kPer; i++) {
+            uint32_t p = threadIdx.x * kPer + i;
             if (p < nc) s.f_pre[p] = excl;
             excl += degs[i];
         }
@@ -377,8 +398,10 @@ __device__ void expand_level(const SegDesc &A, SamplerSmem &s, NodeRec *rec,
     __syncthreads();
 }
 
-__global__ void __launch_bounds__(kSamplerBlock, 2) sampler_kernel(SamplerLaunch L) {
-    __shared__ SamplerSmem s;
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK, Shape<BLOCK>::kMinBlocks) sampler_kernel(SamplerLaunch L) {
+    constexpr int kWarps = Shape<BLOCK>::kWarps;
+    __shared__ SamplerSmem<BLOCK> s;
     const uint32_t slot = blockIdx.x;
     const uint64_t base = (uint64_t)slot * L.slots.stride;
     NodeRec *rec = L.slots.rec + base;
@@ -411,7 +434,7 @@ __global__ void __launch_bounds__(kSamplerBlock, 2) sampler_kernel(SamplerLaunch
         {
             const uint32_t *src = reinterpret_cast<const uint32_t *>(&L.segs[s.sample]);
             uint32_t *dst = reinterpret_cast<uint32_t *>(&s.seg);
-            for (uint32_t i = threadIdx.x; i < sizeof(SegDesc) / 4; i += kSamplerBlock)
+            for (uint32_t i = threadIdx.x; i < sizeof(SegDesc) / 4; i += BLOCK)
                 dst[i] = src[i];
         }
         __syncthreads();
@@ -446,7 +469,9 @@ __global__ void __launch_bounds__(kSamplerBlock, 2) sampler_kernel(SamplerLaunch
                 A.out_status[sl] = 0;
                 A.out_ball[sl] = 0;
                 A.out_pred[sl] = 0;
-                atomicAdd(&L.hdr->cycles, (unsigned long long)(clock64() - t_sample0));
+                const unsigned long long dc = (unsigned long long)(clock64() - t_sample0);
+                atomicAdd(&L.hdr->cycles, dc);
+                atomicMax(&L.hdr->max_cycles, dc);
             }
             __syncthreads();
             continue;
@@ -513,7 +538,7 @@ __global__ void __launch_bounds__(kSamplerBlock, 2) sampler_kernel(SamplerLaunch
             // inclusive prefix of sigma(x) * sigma(y), wrapping; non-decreasing
             // exactly when the 64-bit sum never wrapped
             unsigned long long carry = 0;
-            for (uint32_t c0 = 0; c0 < nm; c0 += kSamplerBlock) {
+            for (uint32_t c0 = 0; c0 < nm; c0 += BLOCK) {
                 uint32_t i = c0 + threadIdx.x;
                 unsigned long long p = 0;
                 if (i < nm) {
@@ -541,7 +566,7 @@ __global__ void __launch_bounds__(kSamplerBlock, 2) sampler_kernel(SamplerLaunch
                 __syncthreads();
             }
             __syncthreads();
-            for (uint32_t i = 1 + threadIdx.x; i < nm; i += kSamplerBlock)
+            for (uint32_t i = 1 + threadIdx.x; i < nm; i += BLOCK)
                 if (__ldcg(&mpre[i]) < __ldcg(&mpre[i - 1])) s.nonmono = 1;
             if (threadIdx.x == 0) s.W = carry;
             __syncthreads();
@@ -568,7 +593,7 @@ __global__ void __launch_bounds__(kSamplerBlock, 2) sampler_kernel(SamplerLaunch
             // ---- paths (:172-197) and backtracks (:241-265) ------------------
             if (s.status == 0 && pl > 0) {
                 const bool mono = s.nonmono == 0;
-                for (uint32_t j = threadIdx.x; j < (uint32_t)np; j += kSamplerBlock) {
+                for (uint32_t j = threadIdx.x; j < (uint32_t)np; j += BLOCK) {
                     uint32_t d = s.draw_base + j * (1u + L);
                     const uint32_t r = (uint32_t)(draw32(A.seed, gidx, d++) % W);
                     uint32_t ei;
@@ -647,7 +672,7 @@ __global__ void __launch_bounds__(kSamplerBlock, 2) sampler_kernel(SamplerLaunch
         __syncthreads();
         const unsigned long long rb = s.rec_base;
         const bool emit = s.status == 0;
-        for (uint32_t i = threadIdx.x; i < nt; i += kSamplerBlock) {
+        for (uint32_t i = threadIdx.x; i < nt; i += BLOCK) {
             const uint32_t a = __ldcg(&touched[i]);
             if (emit) {
                 PathRec pr;
@@ -659,7 +684,7 @@ __global__ void __launch_bounds__(kSamplerBlock, 2) sampler_kernel(SamplerLaunch
             hits[a] = 0;
         }
         const uint32_t eq = s.end_q;
-        for (uint32_t i = threadIdx.x; i < eq; i += kSamplerBlock) rec_reset(&rec[__ldcg(&queue[i])]);
+        for (uint32_t i = threadIdx.x; i < eq; i += BLOCK) rec_reset(&rec[__ldcg(&queue[i])]);
         if (threadIdx.x == 0) {
             A.out_pl[sl] = s.status == 0 ? pl : 0;
             A.out_np[sl] = s.status == 0 ? np : 0;
@@ -667,7 +692,9 @@ __global__ void __launch_bounds__(kSamplerBlock, 2) sampler_kernel(SamplerLaunch
             A.out_status[sl] = s.status;
             A.out_ball[sl] = s.end_q;
             A.out_pred[sl] = s.pred_hits;
-            atomicAdd(&L.hdr->cycles, (unsigned long long)(clock64() - t_sample0));
+            const unsigned long long dc = (unsigned long long)(clock64() - t_sample0);
+            atomicAdd(&L.hdr->cycles, dc);
+            atomicMax(&L.hdr->max_cycles, dc);
         }
         __syncthreads();
     }
@@ -679,6 +706,7 @@ __global__ void round_begin_kernel(SamplerLaunch L, uint32_t max_segs) {
     if (threadIdx.x == 0) {
         L.hdr->work = 0;
         L.hdr->cycles = 0;
+        L.hdr->max_cycles = 0;
     }
 }
 
@@ -703,15 +731,27 @@ cudaError_t sampler_round_begin(const SamplerLaunch &L, uint32_t max_segs, cudaS
     return cudaGetLastError();
 }
 
-cudaError_t sampler_launch(const SamplerLaunch &L, uint32_t grid, cudaStream_t stream) {
+cudaError_t sampler_launch(const SamplerLaunch &L, uint32_t grid, cudaStream_t stream, int block) {
     if (grid == 0) return cudaSuccess;
-    sampler_kernel<<<grid, kSamplerBlock, 0, stream>>>(L);
+    switch (block) {
+    case 128: sampler_kernel<128><<<grid, 128, 0, stream>>>(L); break;
+    case 256: sampler_kernel<256><<<grid, 256, 0, stream>>>(L); break;
+    case 512: sampler_kernel<512><<<grid, 512, 0, stream>>>(L); break;
+    case 1024: sampler_kernel<1024><<<grid, 1024, 0, stream>>>(L); break;
+    default: return cudaErrorInvalidValue;
+    }
     return cudaGetLastError();
 }
 
-int sampler_max_ctas_per_sm() {
+int sampler_max_ctas_per_sm(int block) {
     int n = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, sampler_kernel, kSamplerBlock, 0);
+    switch (block) {
+    case 128: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, sampler_kernel<128>, 128, 0); break;
+    case 256: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, sampler_kernel<256>, 256, 0); break;
+    case 512: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, sampler_kernel<512>, 512, 0); break;
+    case 1024: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, sampler_kernel<1024>, 1024, 0); break;
+    default: break;
+    }
     return n;
 }
 

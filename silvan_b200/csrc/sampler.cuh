@@ -9,7 +9,8 @@
 
 namespace silvan {
 
-constexpr int kSamplerBlock = 512;   // threads per slot
+constexpr int kSamplerBlock = 512;   // default threads per slot
+constexpr int kSamplerBlocks[4] = {128, 256, 512, 1024};  // compiled CTA sizes
 constexpr uint32_t kMeetCap = 1u << 16;  // meeting edges per sample
 
 // One job's share of a sampler launch: samples [first_sample, first_sample +
@@ -49,7 +50,8 @@ struct RoundHeader {
     uint32_t total;   // samples over all segments
     uint32_t work;    // next work index (zeroed by round_begin)
     uint32_t pad;
-    unsigned long long cycles;  // SM cycles spent in samples (zeroed by round_begin)
+    unsigned long long cycles;      // SM cycles spent in samples (zeroed by round_begin)
+    unsigned long long max_cycles;  // cycles of the slowest sample (zeroed by round_begin)
 };
 
 struct SlotArrays {
@@ -74,10 +76,12 @@ cudaError_t sampler_init_slots(NodeRec *rec, uint32_t *hits, uint64_t total_node
 
 // Zeroes the work counter and every segment's record cursor.
 cudaError_t sampler_round_begin(const SamplerLaunch &L, uint32_t max_segs, cudaStream_t stream);
-// Runs the round with `grid` resident CTAs (persistent, work-stealing).
-cudaError_t sampler_launch(const SamplerLaunch &L, uint32_t grid, cudaStream_t stream);
+// Runs the round with `grid` resident CTAs of `block` threads (one of
+// kSamplerBlocks; persistent, work-stealing).
+cudaError_t sampler_launch(const SamplerLaunch &L, uint32_t grid, cudaStream_t stream,
+                           int block = kSamplerBlock);
 
-// Function attributes for the occupancy-based slot choice.
-int sampler_max_ctas_per_sm();
+// Resident CTAs per SM of the `block`-thread sampler (0 for other sizes).
+int sampler_max_ctas_per_sm(int block = kSamplerBlock);
 
 }  // namespace silvan

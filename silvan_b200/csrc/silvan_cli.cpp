@@ -8,7 +8,8 @@
 //
 // Options beyond the reference's (long options, so that the reference's
 // short-option set is unchanged): --plain (one launch sequence per 11-sample
-// block), --seed N (job seed), --np-cap N (paths per sample), --slots N.
+// block), --seed N (job seed), --np-cap N (paths per sample), --slots N,
+// --block N (threads per sampler slot; default autotuned).
 #include <cerrno>
 #include <climits>
 #include <cstdio>
@@ -38,7 +39,7 @@ double peeling_a = 2.0;
 bool m_hat = true;
 bool plain = false;
 uint64_t seed = 42;
-uint32_t np_cap = 0, slots = 0;
+uint32_t np_cap = 0, slots = 0, block = 0;
 
 // silvan/main.cpp:51-68
 void usage(const char *b) {
@@ -64,7 +65,8 @@ void usage(const char *b) {
     std::cerr << "\tgraph: graph edge list file" << std::endl;
     std::cerr << "\t--plain: one launch sequence per 11-sample block (default: batched)"
               << std::endl;
-    std::cerr << "\t--seed N, --np-cap N, --slots N: job seed, paths per sample, sampler slots"
+    std::cerr << "\t--seed N, --np-cap N, --slots N, --block N: job seed, paths per sample, "
+                 "sampler slots, threads per slot"
               << std::endl;
 }
 
@@ -74,6 +76,7 @@ int parse(int argc, char **argv) {
                                        {"seed", required_argument, nullptr, 2},
                                        {"np-cap", required_argument, nullptr, 3},
                                        {"slots", required_argument, nullptr, 4},
+                                       {"block", required_argument, nullptr, 5},
                                        {nullptr, 0, nullptr, 0}};
     int opt;
     while ((opt = getopt_long(argc, argv, "dhmk:o:s:a:v:", longopts, nullptr)) != -1) {
@@ -118,6 +121,7 @@ int parse(int argc, char **argv) {
             case 2: seed = std::strtoull(optarg, nullptr, 10); break;
             case 3: np_cap = (uint32_t)std::strtoul(optarg, nullptr, 10); break;
             case 4: slots = (uint32_t)std::strtoul(optarg, nullptr, 10); break;
+            case 5: block = (uint32_t)std::strtoul(optarg, nullptr, 10); break;
             default: break;
         }
     }
@@ -187,6 +191,7 @@ int main(int argc, char **argv) {
     p.form = plain ? SILVAN_FORM_PLAIN : SILVAN_FORM_BATCHED;
     p.np_cap = np_cap;
     p.slots = slots;
+    p.block = block;
     silvan_job_t j = nullptr;
     rc = silvan_job_create(g, &p, &j);
     if (rc != SILVAN_OK) {
