@@ -59,12 +59,11 @@ struct SamplerSmem {
     uint32_t f_off[kChunk];
     uint32_t f_pre[kChunk + 1];
     unsigned long long f_sig[kChunk];
-    uint32_t warp_a[kWarps];
-    uint32_t warp_b[kWarps];
+    uint32_t warp_a[kItems * kWarps];  // per (item slot, warp): joins, then their offsets
+    uint32_t warp_b[kItems * kWarps];  // per (item slot, warp): meeting edges, offsets
     uint32_t scan_tmp[kWarps + 1];
     unsigned long long wsum[kWarps];
     unsigned long long rec_base;
-    uint32_t tile_n_base, tile_m_base, tile_n_tot, tile_m_tot;
     uint32_t sum_new;
     uint32_t pred_hits;
     // sample state
@@ -93,6 +92,11 @@ __device__ __forceinline__ uint32_t lanemask_lt() {
 
 __device__ __forceinline__ uint32_t draw32(uint64_t seed, uint32_t sample, uint32_t d) {
     return philox_lo32(seed, sample, kStreamSampler, d);
+}
+
+// x mod m for a 32-bit x and a non-zero 64-bit m: x itself when m >= 2^32.
+__device__ __forceinline__ uint32_t mod_u64(uint32_t x, unsigned long long m) {
+    return (m >> 32) ? x : x % (uint32_t)m;
 }
 
 // Exclusive block scan of one value per thread; returns the block total.
@@ -217,16 +221,14 @@ __device__ uint32_t middle_pred(const SegDesc &A, const Smem &s, const NodeRec *
     return bx;
 }
 
-template <class Smem>
-__device__ __forceinline__ void note_hit(uint32_t *hits, uint32_t *touched, Smem &s,
-                                         uint32_t a) {
-    if (atomicAdd(&hits[a], 1u) == 0u) {
-        uint32_t i = atomicAdd(&s.ntouched, 1u);
-        touched[i] = a;
-    }
-}
-
 // Expands one BFS level of `side` (silvan/src/Sp_sampler.cpp:89-143).
+//
+// The level is latency-bound on deep, narrow searches (a grid's ~200 levels
+// of a few hundred nodes), so every phase first issues all of its
+// independent global loads (read-only CSR through the non-coherent path, slot
+// state through L2) and only then stores or issues atomics: a store between
+// two loads would serialise them, because the compiler cannot prove that they
+// do not alias.
 template <int BLOCK>
 __device__ void expand_level(const SegDesc &A, SamplerSmem<BLOCK> &s, NodeRec *rec,
                              uint32_t *queue, uint2 *meet, uint32_t side, uint32_t lo,
@@ -245,139 +247,189 @@ __device__ void expand_level(const SegDesc &A, SamplerSmem<BLOCK> &s, NodeRec *r
     for (uint32_t c0 = lo; c0 < hi; c0 += kChunk) {
         const uint32_t nc = min((uint32_t)kChunk, hi - c0);
         // stage the chunk: row starts, degrees (prefix), sigma
-        uint32_t degs[kPer];
+        uint32_t xq[kPer], o0[kPer], o1[kPer];
+        unsigned long long sg[kPer];
+#pragma unroll
+        for (int i = 0; i < kPer; i++) {
+            const uint32_t p = threadIdx.x * kPer + i;
+            xq[i] = p < nc ? __ldcg(&queue[c0 + p]) : 0u;
+        }
+#pragma unroll
+        for (int i = 0; i < kPer; i++) {
+            const uint32_t p = threadIdx.x * kPer + i;
+            o0[i] = o1[i] = 0;
+            sg[i] = 0;
+            if (p < nc) {
+                o0[i] = __ldg(&off[xq[i]]);
+                o1[i] = __ldg(&off[xq[i] + 1]);
+                sg[i] = __ldcg(&rec[xq[i]].sigma);
+            }
+        }
         uint32_t tsum = 0;
 #pragma unroll
         for (int i = 0; i < kPer; i++) {
-            uint32_t p = threadIdx.x * kPer + i;
-            uint32_t d = 0;
+            const uint32_t p = threadIdx.x * kPer + i;
             if (p < nc) {
-                uint32_t x = __ldcg(&queue[c0 + p]);
-                uint32_t o0 = off[x];
-                d = off[x + 1] - o0;
-                s.f_node[p] = x;
-                s.f_off[p] = o0;
-                s.f_sig[p] = __ldcg(&rec[x].sigma);
+                s.f_node[p] = xq[i];
+                s.f_off[p] = o0[i];
+                s.f_sig[p] = sg[i];
             }
-            degs[i] = d;
-            tsum += d;
+            tsum += o1[i] - o0[i];
         }
         uint32_t excl;
         uint32_t total = block_exclusive_scan<BLOCK>(tsum, excl, s.scan_tmp);
 #pragma unroll
         for (int i = 0; i < kPer; i++) {
-            uint32_t p = threadIdx.x * kPer + i;
+            const uint32_t p = threadIdx.x * kPer + i;
             if (p < nc) s.f_pre[p] = excl;
-            excl += degs[i];
+            excl += o1[i] - o0[i];
         }
         if (threadIdx.x == 0) s.f_pre[nc] = total;
         __syncthreads();
         const uint32_t G = total;
         for (uint32_t t0 = 0; t0 < G; t0 += kTile) {
             // ---- phase 1 ------------------------------------------------------
-            uint32_t ys[kItems], xs[kItems], code[kItems];
+            // item slot k of thread tid is item t0 + k * BLOCK + tid: a narrow
+            // level spreads over every warp, and the item order is (k, warp, lane)
+            uint32_t ys[kItems], xs[kItems], code[kItems], li[kItems];
 #pragma unroll
             for (int k = 0; k < kItems; k++) {
-                uint32_t it = t0 + (uint32_t)(warp * 32 * kItems + k * 32 + lane);
+                const uint32_t it = t0 + (uint32_t)(k * BLOCK) + threadIdx.x;
                 code[k] = 0;
                 ys[k] = 0;
                 xs[k] = 0;
+                li[k] = 0;
                 if (it < G) {
                     uint32_t l = 0, h = nc;
                     while (h - l > 1) {
-                        uint32_t mid = (l + h) >> 1;
+                        const uint32_t mid = (l + h) >> 1;
                         if (s.f_pre[mid] <= it) l = mid;
                         else h = mid;
                     }
-                    const uint32_t x = s.f_node[l];
-                    const uint32_t y = adj[s.f_off[l] + (it - s.f_pre[l])];
-                    xs[k] = x;
-                    ys[k] = y;
-                    // unvisited, or joined earlier in this level: a new-level
-                    // hit (the joining hit marks the node in phase 2)
-                    const uint32_t sty = __ldcg(&rec[y].st);
-                    if (sty == 0u || sty == new_st) {
-                        code[k] = 1;
-                    } else if (st_side(sty) != side) {
-                        code[k] = 2;
-                    }
-                    if (code[k] == 1) {
-                        const unsigned long long key =
-                            ((unsigned long long)(gbase + it) << 32) | x;
-                        atomicMin(reinterpret_cast<unsigned long long *>(&rec[y].first), key);
-                        atomicMax(reinterpret_cast<unsigned long long *>(&rec[y].last), key);
-                        atomicAdd(&rec[y].cnt, 1u);
-                        atomicAdd(reinterpret_cast<unsigned long long *>(&rec[y].sigma),
-                                  s.f_sig[l]);
-                    }
+                    li[k] = l;
+                    xs[k] = s.f_node[l];
+                    ys[k] = __ldg(&adj[s.f_off[l] + (it - s.f_pre[l])]);
+                    code[k] = 3;  // valid, state not read yet
                 }
+            }
+            uint32_t sty[kItems];
+#pragma unroll
+            for (int k = 0; k < kItems; k++) sty[k] = code[k] ? __ldcg(&rec[ys[k]].st) : 0u;
+#pragma unroll
+            for (int k = 0; k < kItems; k++) {
+                if (!code[k]) continue;
+                // unvisited, or joined earlier in this level: a new-level hit
+                // (the joining hit marks the node in phase 2)
+                if (sty[k] == 0u || sty[k] == new_st) code[k] = 1;
+                else if (st_side(sty[k]) != side) code[k] = 2;
+                else code[k] = 0;
+            }
+#pragma unroll
+            for (int k = 0; k < kItems; k++) {
+                if (code[k] != 1) continue;
+                const uint32_t it = t0 + (uint32_t)(k * BLOCK) + threadIdx.x;
+                const unsigned long long key = ((unsigned long long)(gbase + it) << 32) | xs[k];
+                NodeRec *r = &rec[ys[k]];
+                atomicMin(reinterpret_cast<unsigned long long *>(&r->first), key);
+                atomicMax(reinterpret_cast<unsigned long long *>(&r->last), key);
+                atomicAdd(&r->cnt, 1u);
+                atomicAdd(reinterpret_cast<unsigned long long *>(&r->sigma), s.f_sig[li[k]]);
             }
             __syncthreads();
             // ---- phase 2: ordered compaction of joins and meeting edges -------
-            uint32_t rn[kItems], rm[kItems];
-            uint32_t cn = 0, cm = 0;
-            uint32_t nhit = 0;
+            unsigned long long fv[kItems];
 #pragma unroll
-            for (int k = 0; k < kItems; k++) nhit += code[k] == 1 ? 1u : 0u;
-            hits_local += nhit;
+            for (int k = 0; k < kItems; k++)
+                fv[k] = code[k] == 1
+                            ? __ldcg(reinterpret_cast<const unsigned long long *>(&rec[ys[k]].first))
+                            : 0ull;
+            uint32_t rn[kItems], rm[kItems], dg[kItems];
 #pragma unroll
             for (int k = 0; k < kItems; k++) {
-                uint32_t it = t0 + (uint32_t)(warp * 32 * kItems + k * 32 + lane);
-                bool win = false;
+                const uint32_t it = t0 + (uint32_t)(k * BLOCK) + threadIdx.x;
                 if (code[k] == 1) {
-                    unsigned long long f = __ldcg(
-                        reinterpret_cast<const unsigned long long *>(&rec[ys[k]].first));
-                    win = (uint32_t)(f >> 32) == gbase + it;
+                    hits_local++;
+                    if ((uint32_t)(fv[k] >> 32) != gbase + it) code[k] = 0;
                 }
-                if (!win && code[k] == 1) code[k] = 0;
-                uint32_t bn = __ballot_sync(0xffffffffu, win);
-                uint32_t bm = __ballot_sync(0xffffffffu, code[k] == 2);
-                rn[k] = cn + __popc(bn & lanemask_lt());
-                rm[k] = cm + __popc(bm & lanemask_lt());
-                cn += __popc(bn);
-                cm += __popc(bm);
             }
-            if (lane == 0) {
-                s.warp_a[warp] = cn;
-                s.warp_b[warp] = cm;
+            // degrees of the joining nodes, loaded before the ordered scan
+#pragma unroll
+            for (int k = 0; k < kItems; k++) {
+                dg[k] = 0;
+                if (code[k] == 1) dg[k] = __ldg(&off[ys[k] + 1]) - __ldg(&off[ys[k]]);
+            }
+#pragma unroll
+            for (int k = 0; k < kItems; k++) {
+                const uint32_t bn = __ballot_sync(0xffffffffu, code[k] == 1);
+                const uint32_t bm = __ballot_sync(0xffffffffu, code[k] == 2);
+                rn[k] = __popc(bn & lanemask_lt());
+                rm[k] = __popc(bm & lanemask_lt());
+                if (lane == 0) {
+                    s.warp_a[k * kWarps + warp] = __popc(bn);
+                    s.warp_b[k * kWarps + warp] = __popc(bm);
+                }
             }
             __syncthreads();
-            if (threadIdx.x == 0) {
-                uint32_t an = 0, am = 0;
-                for (int w = 0; w < kWarps; w++) {
-                    uint32_t tn = s.warp_a[w], tm = s.warp_b[w];
-                    s.warp_a[w] = an;
-                    s.warp_b[w] = am;
-                    an += tn;
-                    am += tm;
+            if (warp == 0) {
+                // exclusive offsets over (k, warp) in item order; the tile's
+                // bases; the queue and meeting-list ends advance here (the
+                // next tile reads them only after its own phase-1 barrier)
+                constexpr int kE = kItems * kWarps;
+                constexpr int kPerLane = (kE + 31) / 32;
+                uint32_t va[kPerLane], vb[kPerLane];
+                uint32_t sa = 0, sb = 0;
+#pragma unroll
+                for (int i = 0; i < kPerLane; i++) {
+                    const int e = lane * kPerLane + i;
+                    va[i] = e < kE ? s.warp_a[e] : 0u;
+                    vb[i] = e < kE ? s.warp_b[e] : 0u;
+                    sa += va[i];
+                    sb += vb[i];
                 }
-                s.tile_n_base = s.end_q;
-                s.tile_m_base = s.nmeet;
-                s.tile_n_tot = an;
-                s.tile_m_tot = am;
-                if (s.nmeet + am > kMeetCap && s.status == 0) s.status = SILVAN_E_CAPACITY;
+                uint32_t ia = sa, ib = sb;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const uint32_t ta = __shfl_up_sync(0xffffffffu, ia, o);
+                    const uint32_t tb = __shfl_up_sync(0xffffffffu, ib, o);
+                    if (lane >= o) {
+                        ia += ta;
+                        ib += tb;
+                    }
+                }
+                const uint32_t an = __shfl_sync(0xffffffffu, ia, 31);
+                const uint32_t am = __shfl_sync(0xffffffffu, ib, 31);
+                const uint32_t qb = s.end_q, mb0 = s.nmeet;
+                __syncwarp();
+                uint32_t ea = qb + ia - sa, eb = mb0 + ib - sb;
+#pragma unroll
+                for (int i = 0; i < kPerLane; i++) {
+                    const int e = lane * kPerLane + i;
+                    if (e < kE) {
+                        s.warp_a[e] = ea;
+                        s.warp_b[e] = eb;
+                    }
+                    ea += va[i];
+                    eb += vb[i];
+                }
+                if (lane == 0) {
+                    s.end_q = qb + an;
+                    s.nmeet = min(mb0 + am, kMeetCap);
+                    if (mb0 + am > kMeetCap && s.status == 0) s.status = SILVAN_E_CAPACITY;
+                }
             }
             __syncthreads();
-            const uint32_t nb = s.tile_n_base + s.warp_a[warp];
-            const uint32_t mb = s.tile_m_base + s.warp_b[warp];
 #pragma unroll
             for (int k = 0; k < kItems; k++) {
                 if (code[k] == 1) {
                     const uint32_t y = ys[k];
-                    queue[nb + rn[k]] = y;
+                    queue[s.warp_a[k * kWarps + warp] + rn[k]] = y;
                     rec[y].st = new_st;
-                    sum_local += off[y + 1] - off[y];
+                    sum_local += dg[k];
                 } else if (code[k] == 2) {
-                    uint32_t pos = mb + rm[k];
+                    const uint32_t pos = s.warp_b[k * kWarps + warp] + rm[k];
                     if (pos < kMeetCap) meet[pos] = make_uint2(xs[k], ys[k]);
                 }
             }
-            __syncthreads();
-            if (threadIdx.x == 0) {
-                s.end_q += s.tile_n_tot;
-                s.nmeet = min(s.nmeet + s.tile_m_tot, kMeetCap);
-            }
-            __syncthreads();
         }
         if (threadIdx.x == 0) s.vis += G;
         gbase += G;
@@ -389,13 +441,21 @@ __device__ void expand_level(const SegDesc &A, SamplerSmem<BLOCK> &s, NodeRec *r
         sum_local += __shfl_xor_sync(0xffffffffu, sum_local, o);
         hits_local += __shfl_xor_sync(0xffffffffu, hits_local, o);
     }
-    if (threadIdx.x == 0) s.sum_new = 0;
-    __syncthreads();
     if (lane == 0) {
-        atomicAdd(&s.sum_new, sum_local);
-        atomicAdd(&s.pred_hits, hits_local);
+        s.warp_a[warp] = sum_local;
+        s.warp_b[warp] = hits_local;
     }
     __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t sn = 0, ph = 0;
+        for (int w = 0; w < kWarps; w++) {
+            sn += s.warp_a[w];
+            ph += s.warp_b[w];
+        }
+        s.sum_new = sn;
+        s.pred_hits += ph;
+    }
+    // the caller's thread 0 consumes sum_new before its next barrier
 }
 
 template <int BLOCK>
@@ -595,7 +655,7 @@ __global__ void __launch_bounds__(BLOCK, Shape<BLOCK>::kMinBlocks) sampler_kerne
                 const bool mono = s.nonmono == 0;
                 for (uint32_t j = threadIdx.x; j < (uint32_t)np; j += BLOCK) {
                     uint32_t d = s.draw_base + j * (1u + L);
-                    const uint32_t r = (uint32_t)(draw32(A.seed, gidx, d++) % W);
+                    const uint32_t r = mod_u64(draw32(A.seed, gidx, d++), W);
                     uint32_t ei;
                     if (mono) {  // first i with prefix > r
                         uint32_t l = 0, h = nm - 1;
@@ -614,6 +674,9 @@ __global__ void __launch_bounds__(BLOCK, Shape<BLOCK>::kMinBlocks) sampler_kerne
                     uint32_t starts[2] = {e.x, e.y};
                     for (int h2 = 0; h2 < 2; h2++) {
                         uint32_t a = starts[h2];
+                        // the hit count of the previous node is checked after
+                        // the next record load has been issued
+                        uint32_t pend = 0xffffffffu, pend_old = 1u;
                         for (uint32_t steps = 0;; steps++) {
                             // every step moves one level closer to a root, so a
                             // walk longer than L or an id outside the graph is an
@@ -622,24 +685,32 @@ __global__ void __launch_bounds__(BLOCK, Shape<BLOCK>::kMinBlocks) sampler_kerne
                                 s.status = SILVAN_E_STATE;
                                 break;
                             }
-                            const uint32_t sta = __ldcg(&rec[a].st);
+                            // the whole record (one sector) in one load
+                            const uint4 r0 = __ldcg(reinterpret_cast<const uint4 *>(&rec[a]));
+                            const uint4 r1 = __ldcg(reinterpret_cast<const uint4 *>(&rec[a]) + 1);
+                            if (pend != 0xffffffffu && pend_old == 0u) {
+                                const uint32_t ti = atomicAdd(&s.ntouched, 1u);
+                                touched[ti] = pend;
+                            }
+                            pend = 0xffffffffu;
+                            const uint32_t sta = r0.x;
                             if (st_dist(sta) == 0) break;  // a is u or v
-                            note_hit(hits, touched, s, a);
-                            const unsigned long long sg = __ldcg(&rec[a].sigma);
+                            pend_old = atomicAdd(&hits[a], 1u);
+                            pend = a;
+                            const unsigned long long sg =
+                                (unsigned long long)r0.z | ((unsigned long long)r0.w << 32);
                             uint32_t rr = draw32(A.seed, gidx, d++);
                             if (sg == 0ull) {
                                 s.status = SILVAN_E_OVERFLOW;
                                 break;
                             }
-                            rr = (uint32_t)(rr % sg);
-                            const uint32_t c = __ldcg(&rec[a].cnt);
+                            rr = mod_u64(rr, sg);
+                            const uint32_t c = r0.y;
                             const uint32_t t = min(rr, c - 1u);
                             if (t == 0) {
-                                a = (uint32_t)__ldcg(
-                                    reinterpret_cast<const unsigned long long *>(&rec[a].first));
+                                a = r1.x;  // low word of first: the joining predecessor
                             } else if (t == c - 1u) {
-                                a = (uint32_t)__ldcg(
-                                    reinterpret_cast<const unsigned long long *>(&rec[a].last));
+                                a = r1.z;  // low word of last
                             } else {
                                 int32_t e = 0;
                                 a = middle_pred(A, s, rec, queue, a, sta, t, e);
@@ -648,6 +719,10 @@ __global__ void __launch_bounds__(BLOCK, Shape<BLOCK>::kMinBlocks) sampler_kerne
                                     break;
                                 }
                             }
+                        }
+                        if (pend != 0xffffffffu && pend_old == 0u) {
+                            const uint32_t ti = atomicAdd(&s.ntouched, 1u);
+                            touched[ti] = pend;
                         }
                     }
                 }
@@ -672,19 +747,41 @@ __global__ void __launch_bounds__(BLOCK, Shape<BLOCK>::kMinBlocks) sampler_kerne
         __syncthreads();
         const unsigned long long rb = s.rec_base;
         const bool emit = s.status == 0;
-        for (uint32_t i = threadIdx.x; i < nt; i += BLOCK) {
-            const uint32_t a = __ldcg(&touched[i]);
-            if (emit) {
-                PathRec pr;
-                pr.node = a;
-                pr.sample = sl;
-                pr.count = __ldcg(&hits[a]);
-                A.recs[rb + i] = pr;
+        for (uint32_t i0 = threadIdx.x; i0 < nt; i0 += 4 * BLOCK) {
+            uint32_t a4[4], c4[4];
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const uint32_t i = i0 + j * BLOCK;
+                a4[j] = i < nt ? __ldcg(&touched[i]) : 0u;
             }
-            hits[a] = 0;
+#pragma unroll
+            for (int j = 0; j < 4; j++) c4[j] = i0 + j * BLOCK < nt ? __ldcg(&hits[a4[j]]) : 0u;
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const uint32_t i = i0 + j * BLOCK;
+                if (i >= nt) continue;
+                if (emit) {
+                    PathRec pr;
+                    pr.node = a4[j];
+                    pr.sample = sl;
+                    pr.count = c4[j];
+                    A.recs[rb + i] = pr;
+                }
+                hits[a4[j]] = 0;
+            }
         }
         const uint32_t eq = s.end_q;
-        for (uint32_t i = threadIdx.x; i < eq; i += BLOCK) rec_reset(&rec[__ldcg(&queue[i])]);
+        for (uint32_t i0 = threadIdx.x; i0 < eq; i0 += 4 * BLOCK) {
+            uint32_t q4[4];
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const uint32_t i = i0 + j * BLOCK;
+                q4[j] = i < eq ? __ldcg(&queue[i]) : 0xffffffffu;
+            }
+#pragma unroll
+            for (int j = 0; j < 4; j++)
+                if (q4[j] != 0xffffffffu) rec_reset(&rec[q4[j]]);
+        }
         if (threadIdx.x == 0) {
             A.out_pl[sl] = s.status == 0 ? pl : 0;
             A.out_np[sl] = s.status == 0 ? np : 0;
