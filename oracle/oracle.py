@@ -143,6 +143,8 @@ class Port:
         lib.orc_result_size.restype = C.c_uint64
         for f in ("orc_run_arrays", "orc_run_ranking", "orc_run_sp_lengths", "orc_run_partitions"):
             getattr(lib, f).restype = None
+        lib.orc_brandes.restype = None
+        lib.orc_brandes.argtypes = [C.c_void_p, C.c_void_p]
         assert lib.orc_result_size() == C.sizeof(RunResult)
         self.lib = lib
 
@@ -169,6 +171,12 @@ class PortGraph:
 
     def replay(self, seed, first, count, alpha):
         return _replay(self.port.lib.orc_replay, self.h, seed, first, count, alpha)
+
+    def brandes(self):
+        """Exact normalised betweenness of every node (the ground truth)."""
+        out = np.zeros(self.n, np.float64)
+        self.port.lib.orc_brandes(self.h, _p(out))
+        return out
 
     def run(self, diameter, eps, delta, k=0, alpha=2.3, alpha_given=False, a=2.0, mhat=True,
             seed=42, threads=1):

@@ -721,6 +721,58 @@ void *orc_graph_new(uint32_t n, int directed, const uint64_t *out_off, const uin
 
 void orc_graph_free(void *g) { delete (OGraph *)g; }
 
+// Exact betweenness (Brandes, "A faster algorithm for betweenness
+// centrality", J. Math. Sociol. 2001) normalised the way SILVAN estimates it:
+// the sum over ordered pairs (s, t), s != t, of sigma_st(v) / sigma_st,
+// divided by n (n - 1).  Path counts are doubles.  The reference has no exact
+// algorithm of its own; this is the ground truth of the (eps, delta) check.
+void orc_brandes(void *gp, double *bc) {
+    const OGraph &g = *(const OGraph *)gp;
+    const uint32_t n = g.n;
+    std::vector<double> acc(n, 0.0);
+#pragma omp parallel
+    {
+        std::vector<double> local(n, 0.0), sigma(n), delta(n);
+        std::vector<int64_t> dist(n);
+        std::vector<uint32_t> order;
+        order.reserve(n);
+#pragma omp for schedule(dynamic, 16)
+        for (int64_t s = 0; s < (int64_t)n; s++) {
+            std::fill(sigma.begin(), sigma.end(), 0.0);
+            std::fill(delta.begin(), delta.end(), 0.0);
+            std::fill(dist.begin(), dist.end(), -1);
+            order.clear();
+            sigma[s] = 1.0;
+            dist[s] = 0;
+            order.push_back((uint32_t)s);
+            for (size_t h = 0; h < order.size(); h++) {
+                const uint32_t x = order[h];
+                for (uint64_t e = g.out_off[x]; e < g.out_off[x + 1]; e++) {
+                    const uint32_t y = g.out_adj[e];
+                    if (dist[y] < 0) {
+                        dist[y] = dist[x] + 1;
+                        order.push_back(y);
+                    }
+                    if (dist[y] == dist[x] + 1) sigma[y] += sigma[x];
+                }
+            }
+            for (size_t h = order.size(); h-- > 1;) {
+                const uint32_t y = order[h];
+                for (uint64_t e = g.ioff()[y]; e < g.ioff()[y + 1]; e++) {
+                    const uint32_t x = g.iadj()[e];
+                    if (dist[x] >= 0 && dist[x] + 1 == dist[y])
+                        delta[x] += sigma[x] / sigma[y] * (1.0 + delta[y]);
+                }
+                local[y] += delta[y];
+            }
+        }
+#pragma omp critical
+        for (uint32_t v = 0; v < n; v++) acc[v] += local[v];
+    }
+    const double norm = (double)n * (double)(n - 1);
+    for (uint32_t v = 0; v < n; v++) bc[v] = acc[v] / norm;
+}
+
 // Per-sample replay of samples [first, first+count).  Entries are the
 // (node, count) pairs of each sample in ascending node order.  Returns the
 // number of entries, -1 if ent_cap is too small, -2 on a zero modulus.

@@ -1,0 +1,43 @@
+"""The (eps, delta) guarantee on the Barabasi-Albert benchmark graph (n =
+10,000, 5 edges per new node, seed 1; eps 0.01, delta 0.05, alpha 2.3,
+a 2, m_hat on, absolute mode): over 20 seeds, the estimates of every node lie
+within eps of the exact betweenness (Brandes, from the oracle) in at least
+(1 - delta) of the runs, i.e. at most one run of 20 may miss."""
+import numpy as np
+import pytest
+
+EPS, DELTA, SEEDS = 0.01, 0.05, 20
+
+
+@pytest.fixture(scope="module")
+def ba10k(sb, port):
+    hg = sb.HostGraph.from_pairs(sb.barabasi_albert(10000, 5, 1), False)
+    csr = hg.csr()
+    bc = port.graph(csr.n, False, csr.out_off, csr.out_adj, csr.in_off, csr.in_adj,
+                    csr.cc).brandes()
+    return hg, csr, bc
+
+
+@pytest.mark.gpu
+def test_device_estimates_within_eps(sb, ba10k):
+    hg, csr, bc = ba10k
+    g = sb.Graph.from_host(hg)
+    errs = []
+    for seed in range(SEEDS):
+        job = sb.Probabilistic(g, EPS, DELTA, seed=1000 + seed)
+        job.run()
+        errs.append(float(np.abs(job.get_centrality() - bc).max()))
+    misses = sum(e > EPS for e in errs)
+    assert misses <= int(DELTA * SEEDS), errs
+
+
+def test_oracle_estimates_within_eps(port, ba10k):
+    """The same check on the CPU restatement (fewer seeds): the algorithm as
+    restated gives the guarantee."""
+    _, csr, bc = ba10k
+    pg = port.graph(csr.n, False, csr.out_off, csr.out_adj, csr.in_off, csr.in_adj, csr.cc)
+    errs = []
+    for seed in range(5):
+        o = pg.run(csr.diameter, EPS, DELTA, seed=2000 + seed)
+        errs.append(float(np.abs(o["approx"] / o["num_samples"] - bc).max()))
+    assert max(errs) <= EPS, errs

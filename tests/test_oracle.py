@@ -97,3 +97,77 @@ def test_port_matches_reference_sources(ref, port, sb, tmp_path, seed):
         rb = pg.run(D, 0.05, 0.1, seed=seed)
         for f in ("approx", "wimpy", "mcrade", "partition_index"):
             np.testing.assert_array_equal(ra[f], rb[f])
+
+
+def _pair_dependencies(n, adj):
+    """sum over ordered pairs (s, t) of sigma_st(v) / sigma_st by explicit
+    BFS path counting from both ends (small graphs only)."""
+    from collections import deque
+
+    def bfs(s):
+        dist = [-1] * n
+        sig = [0] * n
+        dist[s], sig[s] = 0, 1
+        q = deque([s])
+        while q:
+            x = q.popleft()
+            for y in adj[x]:
+                if dist[y] < 0:
+                    dist[y] = dist[x] + 1
+                    q.append(y)
+                if dist[y] == dist[x] + 1:
+                    sig[y] += sig[x]
+        return dist, sig
+
+    radj = [[] for _ in range(n)]
+    for x in range(n):
+        for y in adj[x]:
+            radj[y].append(x)
+    fw = [bfs(s) for s in range(n)]
+
+    def bfs_rev(t):
+        dist = [-1] * n
+        sig = [0] * n
+        dist[t], sig[t] = 0, 1
+        q = deque([t])
+        while q:
+            x = q.popleft()
+            for y in radj[x]:
+                if dist[y] < 0:
+                    dist[y] = dist[x] + 1
+                    q.append(y)
+                if dist[y] == dist[x] + 1:
+                    sig[y] += sig[x]
+        return dist, sig
+
+    bw = [bfs_rev(t) for t in range(n)]
+    bc = np.zeros(n)
+    for s in range(n):
+        ds, ss = fw[s]
+        for t in range(n):
+            if t == s or ds[t] < 0:
+                continue
+            dt, st = bw[t]
+            for v in range(n):
+                if v in (s, t) or ds[v] < 0 or dt[v] < 0:
+                    continue
+                if ds[v] + dt[v] == ds[t]:
+                    bc[v] += ss[v] * st[v] / ss[t]
+    return bc / (n * (n - 1))
+
+
+@pytest.mark.parametrize("directed", [False, True])
+def test_brandes_matches_pair_enumeration(sb, port, directed):
+    """The exact-betweenness ground truth of the (eps, delta) check."""
+    pairs = sb.rmat(5, 3, 17, directed) if directed else sb.barabasi_albert(28, 2, 17)
+    hg = sb.HostGraph.from_pairs(pairs, directed)
+    csr = hg.csr()
+    adj = [list(csr.out_adj[csr.out_off[u]:csr.out_off[u + 1]]) for u in range(csr.n)]
+    want = _pair_dependencies(csr.n, adj)
+    got = port.graph(csr.n, csr.directed, csr.out_off, csr.out_adj, csr.in_off, csr.in_adj,
+                     csr.cc).brandes()
+    np.testing.assert_allclose(got, want, rtol=1e-12, atol=1e-15)
+    # a path 0-1-2: the middle node lies on both ordered pairs (0,2), (2,0)
+    p3 = sb.HostGraph.from_pairs(np.array([[0, 1], [1, 2]], np.uint32), False).csr()
+    b3 = port.graph(p3.n, False, p3.out_off, p3.out_adj, p3.in_off, p3.in_adj, p3.cc).brandes()
+    np.testing.assert_allclose(b3, [0, 1 / 3, 0])
