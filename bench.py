@@ -20,8 +20,14 @@ reference reports as "Total time".  time-to-(eps,delta) is reported beside it.
           the reference's own estimator (silvan/src/*.cpp with its LCG and
           OpenMP, its own flags) on the same graph, all host threads
 
+Other workloads (--config): ba10k (Barabasi-Albert n = 10^4), grid2048 (top-10
+on a 2048 x 2048 lattice with shortcuts), multigraph64 (64 graphs of uneven
+size in one batched run), serve (a Poisson stream of requests on fresh R-MAT
+graphs: p50/p99 latency and paths/s under continuous batching).
+
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                       [--config rmat20|ba10k] [--form batched|plain]
+                       [--config rmat20|ba10k|grid2048|multigraph64|serve]
+                       [--form batched|plain] [--block 0|128|256|512|1024]
 """
 from __future__ import annotations
 
@@ -39,10 +45,27 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 CONFIGS = {
-    "rmat20": dict(workload="rmat20_directed_ef16_seed2", gen="rmat", scale=20, edge_factor=16,
-                   seed=2, directed=True, eps=0.005, delta=0.05, k=0),
-    "ba10k": dict(workload="ba_n10000_m5_seed1", gen="ba", n=10000, m=5, seed=1,
+    # R-MAT scale 20: the headline configuration (batched vs plain)
+    "rmat20": dict(kind="single", workload="rmat20_directed_ef16_seed2", gen="rmat", scale=20,
+                   edge_factor=16, seed=2, directed=True, eps=0.005, delta=0.05, k=0),
+    # Barabasi-Albert n = 10^4: the CPU-runnable case, checked against Brandes
+    "ba10k": dict(kind="single", workload="ba_n10000_m5_seed1", gen="ba", n=10000, m=5, seed=1,
                   directed=False, eps=0.01, delta=0.05, k=0),
+    # 2048 x 2048 grid, 5 % of edges deleted, 0.1 % shortcuts: top-10 relative
+    # mode with single-path sampling (-s 0); the reference's default alpha
+    # makes path counts explode on lattices (reported beside the line)
+    "grid2048": dict(kind="single", workload="grid2048_del05_short001_seed3_top10", gen="grid",
+                     side=2048, delete=0.05, shortcut=0.001, seed=3, directed=False, eps=0.1,
+                     delta=0.05, k=10, alpha=0.0, alpha_given=True, cpu_samples=40000),
+    # 64 graphs of uneven size (half ER mean degree 8, half BA 4 edges per
+    # node, n log-uniform in [10^3, 2 * 10^6], seeds 100-163) in one batched run
+    "multigraph64": dict(kind="multi", workload="64_graphs_er8_ba4_n1e3_2e6_seeds100_163",
+                         eps=0.01, delta=0.05),
+    # Poisson request stream of fresh R-MAT graphs (scale 10-20, directed
+    # with probability 1/2, eps in {0.01, 0.005, 0.0025}, top-10 on 20 %; the
+    # top-10 requests take their relative eps as 10 x that draw: at relative
+    # eps 0.01 one scale-20 top-10 request alone needs over 4 * 10^7 samples)
+    "serve": dict(kind="serve", workload="rmat_scale10_20_poisson_stream", delta=0.05),
 }
 
 
@@ -59,9 +82,32 @@ def make_graph(cfg):
     import silvan_b200 as sb
     if cfg["gen"] == "rmat":
         pairs = sb.rmat(cfg["scale"], cfg["edge_factor"], cfg["seed"], cfg["directed"])
+    elif cfg["gen"] == "grid":
+        pairs = sb.grid(cfg["side"], cfg["delete"], cfg["shortcut"], cfg["seed"])
     else:
         pairs = sb.barabasi_albert(cfg["n"], cfg["m"], cfg["seed"])
     return sb.HostGraph.from_pairs(pairs, cfg["directed"])
+
+
+def multigraph_hosts():
+    """The 64 graphs of the multi-graph workload."""
+    import math
+
+    import numpy as np
+    import silvan_b200 as sb
+    out = []
+    for i in range(64):
+        seed = 100 + i
+        rng = np.random.default_rng(seed)
+        n = int(round(math.exp(rng.uniform(math.log(1e3), math.log(2e6)))))
+        pairs = sb.erdos_renyi(n, 8.0, seed) if i % 2 == 0 else sb.barabasi_albert(n, 4, seed)
+        out.append(sb.HostGraph.from_pairs(pairs, False))
+    return out
+
+
+def job_kwargs(cfg):
+    return dict(k=cfg.get("k", 0), alpha=cfg.get("alpha", 2.3),
+                alpha_given=cfg.get("alpha_given", False))
 
 
 class ClockSampler:
@@ -128,19 +174,51 @@ def refbench_lib():
     lib.refbench_run.argtypes = [C.c_uint32, C.c_int] + [C.c_void_p] * 4 + \
         [C.c_double, C.c_double, C.c_uint32, C.c_double, C.c_int, C.c_double, C.c_int, C.c_int] + \
         [C.c_void_p] * 5 + [C.c_uint64]
+    lib.refbench_sample.restype = C.c_int
+    lib.refbench_sample.argtypes = [C.c_uint32, C.c_int] + [C.c_void_p] * 4 + \
+        [C.c_double, C.c_int, C.c_uint64, C.c_void_p, C.c_void_p, C.c_void_p]
     return lib
 
 
 def reference_run(lib, csr, cfg, threads):
     tt, p1, p2, vis = C.c_double(), C.c_uint64(), C.c_uint64(), C.c_uint64()
+    kw = job_kwargs(cfg)
     rc = lib.refbench_run(csr.n, int(csr.directed), csr.out_off.ctypes.data,
                           csr.out_adj.ctypes.data, csr.in_off.ctypes.data,
-                          csr.in_adj.ctypes.data, cfg["eps"], cfg["delta"], cfg["k"], 2.3, 0,
-                          2.0, 1, threads, C.byref(tt), C.byref(p1), C.byref(p2), C.byref(vis),
-                          None, 0)
+                          csr.in_adj.ctypes.data, cfg["eps"], cfg["delta"], kw["k"], kw["alpha"],
+                          int(kw["alpha_given"]), 2.0, 1, threads, C.byref(tt), C.byref(p1),
+                          C.byref(p2), C.byref(vis), None, 0)
     if rc != 0:
         raise RuntimeError("reference run failed")
     return dict(total_time=tt.value, samples=p1.value + p2.value, vis=vis.value)
+
+
+def reference_sample(lib, csr, cfg, threads, count):
+    """A bounded sample of the reference's per-sample routine (random_path)
+    on all threads: samples per second of the parallel region."""
+    sec, vis, paths = C.c_double(), C.c_uint64(), C.c_uint64()
+    rc = lib.refbench_sample(csr.n, int(csr.directed), csr.out_off.ctypes.data,
+                             csr.out_adj.ctypes.data, csr.in_off.ctypes.data,
+                             csr.in_adj.ctypes.data, job_kwargs(cfg)["alpha"], threads, count,
+                             C.byref(sec), C.byref(vis), C.byref(paths))
+    if rc != 0:
+        raise RuntimeError("reference sample failed")
+    return dict(total_time=sec.value, samples=count, vis=vis.value)
+
+
+def cpu_reference(lib, csr, cfg, threads):
+    """The reference on the workload's graph, bounded to seconds: a whole
+    estimation where one takes seconds, else a sample of random_path calls."""
+    if cfg.get("cpu_samples"):
+        r = reference_sample(lib, csr, cfg, threads, cfg["cpu_samples"])
+        what = (f"{cfg['cpu_samples']} calls of the reference's random_path (its own LCG, "
+                f"one sampler per OpenMP thread) on the benchmark graph; a whole estimation "
+                f"takes minutes on the host")
+    else:
+        r = reference_run(lib, csr, cfg, threads)
+        what = ("one complete estimation of the benchmark graph by the reference's OpenMP "
+                "build ('Total time' window)")
+    return r, what
 
 
 def dist_env():
@@ -160,27 +238,283 @@ def run_reference_arm(args, cfg):
                           "oracle/_ref/libsilvan_refbench.so was not built (needs the "
                           "reference sources at build time)"}))
         return 0
-    hg = make_graph(cfg)
-    csr = hg.csr()
+    if cfg["kind"] == "serve":
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "the reference has no request server; the serve line carries its "
+                          "CPU baseline"}))
+        return 0
     threads = os.cpu_count() or 1
+    holder = {}
+    if cfg["kind"] == "multi":
+        csrs = [h.csr() for h in multigraph_hosts()[:8]]
+        holder["what"] = "complete estimations of the first 8 of the 64 graphs, one by one"
+
+        def run():
+            return [reference_run(lib, c, cfg, threads) for c in csrs]
+    else:
+        csr = make_graph(cfg).csr()
+
+        def run():
+            r, holder["what"] = cpu_reference(lib, csr, cfg, threads)
+            return [r]
     for _ in range(args.warmup):
-        reference_run(lib, csr, cfg, threads)
-    runs = [reference_run(lib, csr, cfg, threads) for _ in range(args.steps)]
+        run()
+    runs = [r for _ in range(args.steps) for r in run()]
+    what = holder["what"]
     samples = sum(r["samples"] for r in runs)
     t = sum(r["total_time"] for r in runs)
     val = samples / t
     print(json.dumps({
         "impl": "reference", "metric": "paths/sec", "value": val, "unit": "paths/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": 1000 * t / len(runs), "higher_is_better": True, "scaling": "weak",
+        "ms_per_step": 1000 * t / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u32/u64/f64", "data": "synthetic",
-        "config": {"workload": cfg["workload"], "eps": cfg["eps"], "delta": cfg["delta"]},
-        "time_to_guarantee_ms": 1000 * t / len(runs),
+        "config": {"workload": cfg["workload"], "eps": cfg.get("eps"), "delta": cfg["delta"]},
+        "time_to_guarantee_ms": 1000 * t / args.steps,
         "cpu_baseline": {"value": val, "unit": "paths/s", "cores": threads, "kind": "reference",
-                         "sample": f"{len(runs)} complete estimations (reference 'Total time' "
-                                   f"window) on the benchmark graph"},
+                         "sample": f"{args.steps} x ({what})"},
         "e2e": {"value": val, "unit": "paths/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
+    }))
+    return 0
+
+
+def default_alpha_probe(sb, g, cfg):
+    """The same job at the reference's default alpha (2.3, not given): on a
+    lattice the multi-path count alpha * W exceeds the per-sample cap, which
+    the library reports instead of looping for hours as the reference does."""
+    t0 = time.perf_counter()
+    try:
+        job = sb.Probabilistic(g, cfg["eps"], cfg["delta"], k=cfg.get("k", 0), seed=7)
+        res = job.run()
+        out = {"status": "ok", "num_samples": res["num_samples"]}
+    except sb.SilvanError as e:
+        out = {"status": "error", "code": e.code, "message": str(e)}
+    out.update(alpha=2.3, seconds=time.perf_counter() - t0)
+    return out
+
+
+def pinned_copy(torch, a):
+    import numpy as np
+    t = torch.empty(a.shape, dtype={np.uint64: torch.int64, np.uint32: torch.int32,
+                                    np.float64: torch.float64}[a.dtype.type], pin_memory=True)
+    v = t.numpy().view(a.dtype)
+    v[...] = a
+    return t, v
+
+
+def pinned_csr(sb, torch, csr, keep):
+    pcsr = sb.CSR(csr.n, csr.directed, *[None] * 5, csr.n_components, csr.diameter)
+    for f in ("out_off", "out_adj", "in_off", "in_adj", "cc"):
+        t, v = pinned_copy(torch, getattr(csr, f))
+        keep.append(t)
+        setattr(pcsr, f, v)
+    return pcsr
+
+
+def csr_bytes(csr):
+    b = int(csr.out_off.nbytes + csr.out_adj.nbytes + csr.cc.nbytes)
+    if csr.directed:
+        b += int(csr.in_off.nbytes + csr.in_adj.nbytes)
+    return b
+
+
+def run_multi(args, cfg):
+    """64 graphs of uneven size estimated together: every round draws the
+    samples of all unfinished jobs in one persistent sampler launch."""
+    rank, _, local = dist_env()
+    if rank != 0:
+        return 0
+    import numpy as np
+    import torch
+    import silvan_b200 as sb
+    torch.cuda.set_device(local)
+    hosts = multigraph_hosts()
+    csrs = [h.csr() for h in hosts]
+    graphs = [sb.Graph.from_host(h) for h in hosts]
+
+    def jobs_for(gs, seed):
+        return [sb.Probabilistic(g, cfg["eps"], cfg["delta"], seed=seed + i,
+                                 block=args.block) for i, g in enumerate(gs)]
+
+    for w in range(args.warmup):
+        sb.run_batched(jobs_for(graphs, 10 * w))
+    torch.cuda.synchronize()
+    times, samples, results = [], 0, []
+    with ClockSampler(local) as clk:
+        for s in range(args.steps):
+            jobs = jobs_for(graphs, 1000 + 100 * s)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            res = sb.run_batched(jobs)
+            torch.cuda.synchronize()
+            times.append(time.perf_counter() - t0)
+            samples += sum(r["first_pass_samples"] + r["num_samples"] for r in res)
+            results.extend(res)
+            del jobs
+    t = sum(times)
+    # the same jobs one after another (each with the whole GPU), for contrast
+    seq_t, seq_samples = 0.0, 0
+    for i, g in enumerate(graphs):
+        job = sb.Probabilistic(g, cfg["eps"], cfg["delta"], seed=1000 + i, block=args.block)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = job.run()
+        torch.cuda.synchronize()
+        seq_t += time.perf_counter() - t0
+        seq_samples += r["first_pass_samples"] + r["num_samples"]
+        del job
+    # e2e: upload of every CSR from pinned host memory, the batched run and
+    # the read-back of every estimate, per step
+    keep = []
+    pcsrs = [pinned_csr(sb, torch, c, keep) for c in csrs]
+    outs = [torch.empty(c.n, dtype=torch.float64, pin_memory=True) for c in csrs]
+    e2e_t, e2e_samples = 0.0, 0
+    for s in range(0 if args.no_e2e else args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        gs = [sb.Graph.upload(pc, with_cc=True) for pc in pcsrs]
+        jobs = jobs_for(gs, 5000 + 100 * s)
+        res = sb.run_batched(jobs)
+        for j, o in zip(jobs, outs):
+            j.get_centrality(out=o.numpy())
+        torch.cuda.synchronize()
+        e2e_t += time.perf_counter() - t0
+        e2e_samples += sum(r["first_pass_samples"] + r["num_samples"] for r in res)
+        del jobs, gs
+    cpu = None
+    if not args.no_cpu_baseline:
+        lib = refbench_lib()
+        if lib is not None:
+            threads = os.cpu_count() or 1
+            rr = [reference_run(lib, c, cfg, threads) for c in csrs[:8]]
+            cpu = {"value": sum(r["samples"] for r in rr) / sum(r["total_time"] for r in rr),
+                   "unit": "paths/s", "cores": threads, "kind": "reference",
+                   "sample": "complete estimations of the first 8 of the 64 graphs by the "
+                             "reference's OpenMP build, one after another"}
+    alg = sum(8 * r["vis_edges"] + 24 * r["ball_nodes"] + 4 * r["pred_entries"] for r in results)
+    print(json.dumps({
+        "metric": "paths/sec", "value": samples / t, "unit": "paths/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * t / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u32/u64/f64", "data": "synthetic",
+        "config": {"workload": cfg["workload"], "graphs": len(graphs),
+                   "nodes_total": int(sum(c.n for c in csrs)),
+                   "edges_total": int(sum(int(c.out_off[-1]) for c in csrs) // 2),
+                   "eps": cfg["eps"], "delta": cfg["delta"], "form": "batched multi-graph",
+                   "timing": "host clock around the batched run, device synchronised on both "
+                             "sides (the jobs run on the engine's own stream)",
+                   "l2": "working set above L2"},
+        "time_to_guarantee_ms": 1000 * t / args.steps,
+        "one_by_one_ms": 1000 * seq_t, "one_by_one_paths_per_s": seq_samples / seq_t,
+        "e2e": {"value": e2e_samples / e2e_t if e2e_t > 0 else None, "unit": "paths/s",
+                "h2d_bytes_per_step": sum(csr_bytes(c) for c in csrs),
+                "d2h_bytes_per_step": sum(c.n * 8 for c in csrs)},
+        "roofline": {"bound": "hbm", "achieved": alg / 1e9 / sum(
+                     r["time_sampling_s"] for r in results) if results[0]["time_sampling_s"]
+                     else None, "peak": peaks()[0], "unit": "GB/s", "frac": None,
+                     "traffic": None, "kernel": "sampler_kernel", "peak_kind": peaks()[1]},
+        "cpu_baseline": cpu,
+        "gpu_launches": sum(r["kernel_launches"] for r in results),
+        "clocks": clk.summary(),
+    }))
+    return 0
+
+
+def run_serve(args, cfg):
+    """A Poisson stream of estimation requests on fresh graphs, served with
+    continuous batching; latency is submission to result."""
+    rank, _, local = dist_env()
+    if rank != 0:
+        return 0
+    import numpy as np
+    import torch
+    import silvan_b200 as sb
+    torch.cuda.set_device(local)
+    hosts = {}
+    for scale in range(10, 21):
+        for d in (0, 1):
+            hosts[(scale, d)] = sb.HostGraph.from_pairs(
+                sb.rmat(scale, 16, 500 + 2 * scale + d, bool(d)), bool(d))
+    rng = np.random.default_rng(5)
+    reqs = []
+    for i in range(args.requests):
+        scale = int(rng.integers(10, 21))
+        d = int(rng.integers(0, 2))
+        eps = float(rng.choice([0.01, 0.005, 0.0025]))
+        k = 10 if rng.random() < 0.2 else 0
+        if k:
+            eps *= 10.0
+        reqs.append((scale, d, eps, k, float(rng.exponential(1.0 / args.rate))))
+    srv = sb.Server(1 << 20, slots=args.slots)
+    try:
+        # warm-up: one request per graph class, one after another
+        for key, hg in hosts.items():
+            srv.wait(srv.submit(hg, 0.01, cfg["delta"], seed=1), 600)
+        ids = [None] * len(reqs)
+        t_first = time.perf_counter()
+
+        def client():
+            t_next = time.perf_counter()
+            for i, (scale, d, eps, k, gap) in enumerate(reqs):
+                t_next += gap
+                dt = t_next - time.perf_counter()
+                if dt > 0:
+                    time.sleep(dt)
+                ids[i] = srv.submit(hosts[(scale, d)], eps, cfg["delta"], k=k, seed=100 + i)
+
+        with ClockSampler(local) as clk:
+            th = threading.Thread(target=client)
+            th.start()
+            th.join()
+            done = [srv.wait(rid, 600) for rid in ids]
+            t_end = time.perf_counter()
+        st = srv.stats()
+    finally:
+        srv.close()
+    lat = np.array([r["latency_s"] for r in done]) * 1000
+    samples = sum(r["first_pass_samples"] + r["num_samples"] for r in done)
+    span = t_end - t_first
+    p50, p99 = float(np.percentile(lat, 50)), float(np.percentile(lat, 99))
+    absolute = np.array([q[3] == 0 for q in reqs])
+    classes = {}
+    for name, mask in (("absolute", absolute), ("top10", ~absolute)):
+        if mask.any():
+            classes[name] = {"requests": int(mask.sum()),
+                             "p50_ms": float(np.percentile(lat[mask], 50)),
+                             "p99_ms": float(np.percentile(lat[mask], 99))}
+    slo_ms = args.slo_ms
+    print(json.dumps({
+        "metric": "serve p99 latency", "value": p99, "unit": "ms", "n_gpus": 1,
+        "steps": len(reqs), "warmup": len(hosts), "ms_per_step": float(lat.mean()),
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u32/u64/f64", "data": "synthetic",
+        "config": {"workload": cfg["workload"], "requests": len(reqs),
+                   "rate_per_s": args.rate, "delta": cfg["delta"],
+                   "graphs": "22 pre-generated R-MAT graphs (scale 10-20 x directed or not), "
+                             "each request uploads and estimates its own copy",
+                   "latency": "host clock from submission to the finished result"},
+        "p50_ms": p50, "p99_ms": p99, "max_ms": float(lat.max()), "by_mode": classes,
+        "slowest": [{"scale": reqs[i][0], "directed": reqs[i][1], "eps": reqs[i][2],
+                     "k": reqs[i][3], "ms": float(lat[i]),
+                     "queued_ms": 1000 * done[i]["queued_s"],
+                     "samples": done[i]["first_pass_samples"] + done[i]["num_samples"]}
+                    for i in np.argsort(-lat)[:6]],
+        "slo": {"p99_ms": slo_ms, "at_rate_per_s": args.rate, "met": p99 <= slo_ms},
+        "paths_per_s": samples / span,
+        "e2e": {"value": samples / span, "unit": "paths/s",
+                "h2d_bytes_per_step": int(np.mean([csr_bytes(hosts[(r[0], r[1])].csr())
+                                                   for r in reqs])),
+                "d2h_bytes_per_step": int(np.mean([8 * hosts[(r[0], r[1])].csr().n
+                                                   for r in reqs]))},
+        "server": {"rounds": st["rounds"], "max_active": st["max_active"],
+                   "slots": st["slots"],
+                   "thread_s": {k: round(st[k + "_s"], 4) for k in
+                                ("admit", "round", "commit", "finish")},
+                   "longest_s": {k: round(st[k + "_max_s"], 4) for k in
+                                 ("admit", "round", "commit", "finish")}},
+        "gpu_launches": int(sum(r["kernel_launches"] for r in done)),
+        "clocks": clk.summary(),
     }))
     return 0
 
@@ -200,10 +534,18 @@ def main():
                          "memory for profiler captures")
     ap.add_argument("--block", type=int, default=0, choices=[0, 128, 256, 512, 1024],
                     help="threads per sampler slot (0 = autotuned per graph and round)")
+    ap.add_argument("--requests", type=int, default=200, help="serve: requests in the stream")
+    ap.add_argument("--rate", type=float, default=4.0, help="serve: Poisson arrivals per second")
+    ap.add_argument("--slo-ms", type=float, default=2500.0,
+                    help="serve: stated p99 objective over all requests")
     args = ap.parse_args()
     cfg = CONFIGS[args.config]
     if args.impl == "reference":
         return run_reference_arm(args, cfg)
+    if cfg["kind"] == "multi":
+        return run_multi(args, cfg)
+    if cfg["kind"] == "serve":
+        return run_serve(args, cfg)
 
     import numpy as np
     import torch
@@ -224,8 +566,8 @@ def main():
     seed0 = 1000 + 100 * rank
 
     def one_run(seed):
-        job = sb.Probabilistic(g, cfg["eps"], cfg["delta"], k=cfg["k"], seed=seed,
-                               form=args.form, slots=args.slots, block=args.block)
+        job = sb.Probabilistic(g, cfg["eps"], cfg["delta"], seed=seed, form=args.form,
+                               slots=args.slots, block=args.block, **job_kwargs(cfg))
         res = job.run()
         del job
         return res
@@ -249,30 +591,17 @@ def main():
 
     # e2e through the C-ABI from pinned host buffers: CSR upload, job
     # creation, the run and the read-back of every estimate, per step
-    def pinned(a):
-        t = torch.empty(a.shape, dtype={np.uint64: torch.int64, np.uint32: torch.int32}[
-            a.dtype.type], pin_memory=True)
-        v = t.numpy().view(a.dtype)
-        v[...] = a
-        return t, v
-
     keep = []
-    pcsr = sb.CSR(csr.n, csr.directed, *[None] * 5, csr.n_components, csr.diameter)
-    for f in ("out_off", "out_adj", "in_off", "in_adj", "cc"):
-        t, v = pinned(getattr(csr, f))
-        keep.append(t)
-        setattr(pcsr, f, v)
+    pcsr = pinned_csr(sb, torch, csr, keep)
     est_t = torch.empty(csr.n, dtype=torch.float64, pin_memory=True)
     e2e_t, e2e_samples = 0.0, 0
-    h2d = int(csr.out_off.nbytes + csr.out_adj.nbytes + csr.cc.nbytes)
-    if csr.directed:
-        h2d += int(csr.in_off.nbytes + csr.in_adj.nbytes)
+    h2d = csr_bytes(csr)
     d2h = csr.n * 8
     for s in range(0 if args.no_e2e else args.steps):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         g2 = sb.Graph.upload(pcsr, with_cc=True)
-        job = sb.Probabilistic(g2, cfg["eps"], cfg["delta"], k=cfg["k"],
+        job = sb.Probabilistic(g2, cfg["eps"], cfg["delta"], **job_kwargs(cfg),
                                seed=seed0 + 50 + s, form=args.form, slots=args.slots,
                                block=args.block)
         r = job.run()
@@ -315,11 +644,9 @@ def main():
             lib = refbench_lib()
             if lib is not None:
                 threads = os.cpu_count() or 1
-                rr = reference_run(lib, csr, cfg, threads)
+                rr, what = cpu_reference(lib, csr, cfg, threads)
                 cpu = {"value": rr["samples"] / rr["total_time"], "unit": "paths/s",
-                       "cores": threads, "kind": "reference",
-                       "sample": "one complete estimation of the benchmark graph by the "
-                                 "reference's OpenMP build ('Total time' window)"}
+                       "cores": threads, "kind": "reference", "sample": what}
         line = {
             "metric": "paths/sec", "value": samples_all / t_max, "unit": "paths/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -328,8 +655,9 @@ def main():
             "data": "synthetic",
             "config": {"workload": cfg["workload"], "n": csr.n, "m": int(csr.out_off[-1]),
                        "eps": cfg["eps"], "delta": cfg["delta"], "form": args.form,
+                       **job_kwargs(cfg),
                        "parallelism": "replicas" if world > 1 else "single",
-                       "l2": "working set above L2 (CSR 128 MB + per-slot state)",
+                       "l2": "working set above L2 (CSR + per-slot state)",
                        "sampler_block": [r["sampler_block"] for r in results],
                        "sampler_launches_per_step": sum(r["sampler_launches"] for r in results)
                        / args.steps},
@@ -356,6 +684,8 @@ def main():
             "gpu_launches": launches,
             "clocks": clk.summary(),
         }
+        if cfg.get("alpha_given") and cfg.get("gen") == "grid":
+            line["default_alpha_run"] = default_alpha_probe(sb, g, cfg)
         print(json.dumps(line))
     if pg:
         pg.barrier()

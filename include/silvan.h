@@ -243,6 +243,11 @@ typedef struct {
     uint64_t budget;        /* admission budget                               */
     uint32_t slots;         /* sampler slots                                  */
     uint32_t pad;
+    /* where the server thread's time went (seconds, totals and the longest
+     * single occurrence): admitting requests (upload, job set-up), sampler
+     * rounds, committing and evaluating, finishing (read-back, release) */
+    double admit_s, round_s, commit_s, finish_s;
+    double admit_max_s, round_max_s, commit_max_s, finish_max_s;
 } silvan_server_stats_t;
 
 /* n_max: largest graph (nodes) the server accepts; the sampler slots are

@@ -128,4 +128,70 @@ extern "C" int refbench_run(uint32_t n, int directed, const uint64_t *out_off,
     return 0;
 }
 
+// A bounded sample of the reference's hot path: `count` calls of its own
+// Sp_sampler::random_path (silvan/src/Sp_sampler.cpp:41-238, its own LCG
+// streams, one sampler per OpenMP thread as in Probabilistic.cpp:825-830) on
+// the CSR graph, timed over the parallel region.  Used where a complete
+// estimation would take minutes on the host (the 2048 x 2048 grid).
+extern "C" int refbench_sample(uint32_t n, int directed, const uint64_t *out_off,
+                               const uint32_t *out_adj, const uint64_t *in_off,
+                               const uint32_t *in_adj, double alpha, int threads,
+                               uint64_t count, double *seconds, uint64_t *vis_edges,
+                               uint64_t *paths) {
+    if (threads > 0) omp_set_num_threads(threads);
+    char path[] = "/tmp/silvan_refbench_XXXXXX";
+    int fd = mkstemp(path);
+    if (fd < 0) return -1;
+    const char two[] = "0 1\n";
+    if (write(fd, two, sizeof(two) - 1) != (ssize_t)(sizeof(two) - 1)) {
+        close(fd);
+        return -1;
+    }
+    close(fd);
+    CoutCapture cap;
+    Graph *g = new Graph(std::string(path), directed != 0);
+    unlink(path);
+    for (uint32_t i = 0; i < g->nodes_num; i++) free(g->adj[i]);
+    free(g->adj);
+    free(g->degrees);
+    if (directed) {
+        for (uint32_t i = 0; i < g->nodes_num; i++) free(g->inc[i]);
+        free(g->inc);
+        free(g->in_degrees);
+    }
+    free(g->cc);
+    g->nodes_num = n;
+    g->edges_num = out_off[n];
+    g->adj = rows(n, out_off, out_adj, &g->degrees);
+    if (directed) {
+        g->inc = rows(n, in_off, in_adj, &g->in_degrees);
+    } else {
+        g->inc = g->adj;
+        g->in_degrees = g->degrees;
+    }
+    g->cc = (uint32_t *)malloc(sizeof(uint32_t) * n);
+    g->estimate_diameter();  // component ids for the void test (outside the timing)
+    uint64_t next = 0, vis = 0, np_total = 0;
+    const double t0 = omp_get_wtime();
+#pragma omp parallel reduction(+ : vis, np_total)
+    {
+        Sp_sampler sp(g, 1234u + 77u * (uint32_t)omp_get_thread_num());
+        for (;;) {
+            uint64_t i;
+#pragma omp atomic capture
+            i = next++;
+            if (i >= count) break;
+            int pl = 0, np = 0;
+            std::map<uint32_t, int> m = sp.random_path(pl, np, alpha);
+            vis += sp.vis_edges;
+            np_total += (uint64_t)(np > 0 ? np : 0);
+        }
+    }
+    *seconds = omp_get_wtime() - t0;
+    *vis_edges = vis;
+    *paths = np_total;
+    delete g;
+    return 0;
+}
+
 extern "C" int refbench_max_threads() { return omp_get_max_threads(); }

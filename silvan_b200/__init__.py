@@ -465,7 +465,11 @@ def run_batched(jobs, mem_budget=0):
 class ServerStats(C.Structure):
     _fields_ = [("rounds", C.c_uint64), ("samples", C.c_uint64), ("max_active", C.c_uint64),
                 ("queued", C.c_uint64), ("active", C.c_uint64), ("bytes_in_use", C.c_uint64),
-                ("budget", C.c_uint64), ("slots", C.c_uint32), ("pad", C.c_uint32)]
+                ("budget", C.c_uint64), ("slots", C.c_uint32), ("pad", C.c_uint32),
+                ("admit_s", C.c_double), ("round_s", C.c_double), ("commit_s", C.c_double),
+                ("finish_s", C.c_double), ("admit_max_s", C.c_double),
+                ("round_max_s", C.c_double), ("commit_max_s", C.c_double),
+                ("finish_max_s", C.c_double)]
 
 
 class Server:

@@ -10,6 +10,7 @@
 #include <map>
 #include <mutex>
 #include <sstream>
+#include <unordered_map>
 
 #include "bounds.h"
 #include "graph_dev.cuh"
@@ -24,13 +25,111 @@ constexpr uint32_t kBlock = 11;  // samples per block (Probabilistic.cpp:829,106
 constexpr uint32_t kUncertainCap = 1u << 16;
 constexpr uint32_t kArgRing = 64;
 
+// Caching allocator for device and pinned host memory.  Requests start and
+// finish all the time in a serving process, and cudaMalloc / cudaFree (and
+// even more so cudaMallocHost / cudaFreeHost) cost milliseconds each, so
+// freed blocks are kept per device and size class and handed out again.  A
+// freed block is reusable only after a device synchronisation (the one
+// cudaFree would have done), taken when a request finds no ready block but
+// freed ones are waiting.  On allocation failure the cached blocks of the
+// device are released and the allocation is tried once more.
+class BlockCache {
+  public:
+    void *alloc(size_t bytes, bool host, cudaError_t *err) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        const size_t cls = size_class(bytes);
+        const Key key{host ? -1 - dev : dev, cls};
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            void *p = take(key);
+            if (!p && !pending_[key].empty()) {
+                cudaDeviceSynchronize();
+                for (auto &kv : pending_) {
+                    auto &f = ready_[kv.first];
+                    f.insert(f.end(), kv.second.begin(), kv.second.end());
+                    kv.second.clear();
+                }
+                p = take(key);
+            }
+            if (p) {
+                live_[p] = key;
+                *err = cudaSuccess;
+                return p;
+            }
+        }
+        void *p = nullptr;
+        *err = host ? cudaMallocHost(&p, cls) : cudaMalloc(&p, cls);
+        if (*err != cudaSuccess) {
+            cudaGetLastError();
+            release(dev);
+            *err = host ? cudaMallocHost(&p, cls) : cudaMalloc(&p, cls);
+            if (*err != cudaSuccess) {
+                cudaGetLastError();
+                return nullptr;
+            }
+        }
+        std::lock_guard<std::mutex> lk(mu_);
+        live_[p] = key;
+        return p;
+    }
+    void free(void *p) {
+        if (!p) return;
+        std::lock_guard<std::mutex> lk(mu_);
+        auto it = live_.find(p);
+        if (it == live_.end()) return;
+        pending_[it->second].push_back(p);
+        live_.erase(it);
+    }
+
+  private:
+    typedef std::pair<int, size_t> Key;  // device (host blocks: -1 - device), class
+    static size_t size_class(size_t b) {
+        if (b <= 256) return 256;
+        if (b <= (2u << 20)) {
+            size_t c = 256;
+            while (c < b) c <<= 1;
+            return c;
+        }
+        return (b + (2u << 20) - 1) & ~(size_t)((2u << 20) - 1);
+    }
+    void *take(const Key &k) {
+        auto it = ready_.find(k);
+        if (it == ready_.end() || it->second.empty()) return nullptr;
+        void *p = it->second.back();
+        it->second.pop_back();
+        return p;
+    }
+    void release(int dev) {
+        std::lock_guard<std::mutex> lk(mu_);
+        cudaDeviceSynchronize();
+        for (auto *m : {&ready_, &pending_})
+            for (auto &kv : *m) {
+                if (kv.first.first != dev && kv.first.first != -1 - dev) continue;
+                for (void *p : kv.second) {
+                    if (kv.first.first < 0) cudaFreeHost(p);
+                    else cudaFree(p);
+                }
+                kv.second.clear();
+            }
+    }
+    std::mutex mu_;
+    std::map<Key, std::vector<void *>> ready_, pending_;
+    std::unordered_map<void *, Key> live_;
+};
+
+BlockCache &block_cache() {
+    static BlockCache *c = new BlockCache();  // outlives every static destructor
+    return *c;
+}
+
 template <typename T>
 int dmalloc(T **p, size_t count) {
     if (count == 0) count = 1;
-    cudaError_t e = cudaMalloc((void **)p, sizeof(T) * count);
+    cudaError_t e;
+    *p = (T *)block_cache().alloc(sizeof(T) * count, false, &e);
     if (e != cudaSuccess) {
         *p = nullptr;
-        cudaGetLastError();
         set_error(std::string("device allocation failed: ") + cudaGetErrorString(e));
         return SILVAN_E_OOM;
     }
@@ -38,24 +137,25 @@ int dmalloc(T **p, size_t count) {
 }
 template <typename T>
 void dfree(T *&p) {
-    if (p) cudaFree((void *)p);
+    block_cache().free((void *)p);
     p = nullptr;
 }
 template <typename T>
 int hmalloc(T **p, size_t count) {
-    cudaError_t e = cudaMallocHost((void **)p, sizeof(T) * std::max<size_t>(count, 1));
+    const size_t bytes = sizeof(T) * std::max<size_t>(count, 1);
+    cudaError_t e;
+    *p = (T *)block_cache().alloc(bytes, true, &e);
     if (e != cudaSuccess) {
         *p = nullptr;
-        cudaGetLastError();
         set_error("pinned host allocation failed");
         return SILVAN_E_OOM;
     }
-    std::memset((void *)*p, 0, sizeof(T) * std::max<size_t>(count, 1));
+    std::memset((void *)*p, 0, bytes);
     return SILVAN_OK;
 }
 template <typename T>
 void hfree(T *&p) {
-    if (p) cudaFreeHost((void *)p);
+    block_cache().free((void *)p);
     p = nullptr;
 }
 }  // namespace
@@ -341,8 +441,8 @@ int Engine::sampler_exec(int block, uint32_t grid, cudaGraphExec_t *out) {
     return SILVAN_OK;
 }
 
-// Autotuned CTA size of a round.  Every CTA size is tried once on each graph
-// (the samples are the same whichever size draws them); after that the round
+// Autotuned CTA size of a round.  Every CTA size is tried once on each class
+// of graphs (the samples are the same whichever size draws them); after that the round
 // takes the size with the least predicted time: the slowest sample of the
 // round, or the CTA time of all its samples spread over the resident CTAs,
 // whichever is longer.
@@ -356,7 +456,7 @@ int Engine::choose_block(const std::vector<Job *> &jobs, const std::vector<JobRe
         const int b = order[oi];
         if (!max_grid_[b]) continue;
         for (uint32_t i : idx) {
-            auto it = stats_.find(jobs[i]->graph()->uid);
+            auto it = stats_.find(jobs[i]->graph()->tune_class());
             if (it == stats_.end() || it->second[b].rounds == 0) return kSamplerBlocks[b];
         }
     }
@@ -366,7 +466,7 @@ int Engine::choose_block(const std::vector<Job *> &jobs, const std::vector<JobRe
         if (!max_grid_[b]) continue;
         double tail = 0, work = 0;
         for (uint32_t i : idx) {
-            const BlockStats &st = stats_.at(jobs[i]->graph()->uid)[b];
+            const BlockStats &st = stats_.at(jobs[i]->graph()->tune_class())[b];
             tail = std::max(tail, st.tail_ms);
             work += reqs[i].count * st.cta_ms;
         }
@@ -379,6 +479,43 @@ int Engine::choose_block(const std::vector<Job *> &jobs, const std::vector<JobRe
     return best;
 }
 
+void Engine::fair_share(const std::vector<Job *> &jobs, std::vector<JobRequest> &reqs,
+                        double round_ms) const {
+    const size_t n = jobs.size();
+    if (n < 2) return;
+    std::vector<double> cost(n, 0.0);
+    uint32_t grid = 0;
+    for (int b = 0; b < kNB; b++) grid = std::max(grid, max_grid_[b]);
+    for (size_t i = 0; i < n; i++) {
+        auto it = stats_.find(jobs[i]->graph()->tune_class());
+        if (it == stats_.end()) return;
+        double best = 0;
+        for (int b = 0; b < kNB; b++) {
+            const BlockStats &st = it->second[b];
+            if (st.rounds && max_grid_[b] && (best == 0 || st.cta_ms / max_grid_[b] < best))
+                best = st.cta_ms / max_grid_[b];
+        }
+        if (best <= 0) return;
+        cost[i] = best * grid;  // CTA ms per sample at the best CTA size
+    }
+    std::vector<size_t> order(n);
+    for (size_t i = 0; i < n; i++) order[i] = i;
+    std::sort(order.begin(), order.end(), [&](size_t a, size_t b) {
+        return reqs[a].count * cost[a] < reqs[b].count * cost[b];
+    });
+    double left = round_ms * grid;
+    for (size_t k = 0; k < n; k++) {
+        const size_t i = order[k];
+        const double share = left / (double)(n - k);
+        const double need = reqs[i].count * cost[i];
+        if (need > share) {
+            const uint32_t c = (uint32_t)std::max<double>(kBlock, std::floor(share / cost[i]));
+            reqs[i].count = std::min(reqs[i].count, c);
+        }
+        left = std::max(0.0, left - reqs[i].count * cost[i]);
+    }
+}
+
 uint32_t Engine::main_block() const {
     int b = 2;
     for (int i = 0; i < kNB; i++)
@@ -386,9 +523,16 @@ uint32_t Engine::main_block() const {
     return (uint32_t)kSamplerBlocks[b];
 }
 
-uint64_t DeviceGraph::next_uid() {
-    static std::atomic<uint64_t> c{1};
-    return c.fetch_add(1);
+uint64_t DeviceGraph::tune_class() const {
+    auto lg = [](uint64_t x) {
+        uint64_t r = 0;
+        while (x > 1) {
+            x >>= 1;
+            r++;
+        }
+        return r;
+    };
+    return (directed ? 1ull : 0ull) | lg(n) << 1 | lg(n ? m / n : 0) << 8;
 }
 
 int Engine::round(const std::vector<Job *> &jobs, const std::vector<JobRequest> &reqs,
@@ -481,7 +625,7 @@ int Engine::round(const std::vector<Job *> &jobs, const std::vector<JobRequest> 
             last_launch_ms_ = ms;
             last_grid_ = grid;
             for (uint32_t i : idx) {
-                BlockStats &st = stats_[jobs[i]->graph()->uid][bi];
+                BlockStats &st = stats_[jobs[i]->graph()->tune_class()][bi];
                 st.cta_ms = st.rounds ? 0.5 * (st.cta_ms + cta_ms) : cta_ms;
                 st.tail_ms = st.rounds ? 0.5 * (st.tail_ms + tail_ms) : tail_ms;
                 st.rounds++;

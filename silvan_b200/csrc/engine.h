@@ -46,8 +46,10 @@ struct DeviceGraph {
     uint32_t *d_in_off = nullptr, *d_in_adj = nullptr;
     uint32_t *d_cc = nullptr;
     int device = 0;
-    uint64_t uid = next_uid();  // keys the sampler's per-graph schedule statistics
-    static uint64_t next_uid();
+    // Class of the graph for the sampler's schedule statistics: graphs with
+    // the same direction, node count and mean degree (both to a power of 2)
+    // share them, so a stream of fresh graphs of a few shapes is tuned once.
+    uint64_t tune_class() const;
 
     int upload();  // from `host` and `cc`
     // from caller-owned host arrays (ideally pinned): copied straight to the
@@ -116,6 +118,13 @@ class Engine {
         block_samples_.fill(0);
     }
     uint32_t sampler_launches() const { return sampler_launches_; }
+    // Shortens the requests of a multi-job round so that the round's
+    // predicted CTA time fits `round_ms` on the resident slots: jobs that
+    // need little get all of it, the rest share what is left evenly (every
+    // job still draws at least one 11-sample block).  Without statistics for
+    // every job's graph class the requests stay as they are.
+    void fair_share(const std::vector<Job *> &jobs, std::vector<JobRequest> &reqs,
+                    double round_ms) const;
     // CTA size that drew the most samples since reset_timers()
     uint32_t main_block() const;
 
@@ -145,7 +154,7 @@ class Engine {
     uint32_t max_segs_ = 0;
     std::vector<Exec> execs_;          // captured round_begin + sampler per (block, grid)
     uint32_t max_grid_[kNB] = {};      // resident CTAs per CTA size (0 = unusable)
-    std::unordered_map<uint64_t, std::array<BlockStats, kNB>> stats_;  // by graph uid
+    std::unordered_map<uint64_t, std::array<BlockStats, kNB>> stats_;  // by tune_class()
     std::array<uint64_t, kNB> block_samples_{};
     uint32_t sampler_launches_ = 0;
     cudaEvent_t ev_[4] = {nullptr, nullptr, nullptr, nullptr};

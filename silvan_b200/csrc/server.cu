@@ -26,6 +26,11 @@
 
 namespace silvan {
 
+// Predicted CTA time of one serving round over all slots: long enough to
+// amortise a launch, short enough that a small request never waits long
+// behind a large one.
+constexpr double kServeRoundMs = 3.0;
+
 struct ServerRequest {
     uint64_t id = 0;
     HostGraph host;
@@ -62,6 +67,15 @@ struct Server {
     std::condition_variable init_cv;
     bool init_done = false;
 
+    // time accounting of the server thread (seconds): total, longest
+    double t_acc[4] = {0, 0, 0, 0}, t_max[4] = {0, 0, 0, 0};
+    void account(int what, double t0) {
+        const double dt = now_seconds() - t0;
+        std::lock_guard<std::mutex> lk(mu);
+        t_acc[what] += dt;
+        t_max[what] = std::max(t_max[what], dt);
+    }
+
     static uint64_t job_bytes(uint64_t n, uint64_t D) {
         // counters + node buckets + round buffers at their initial capacity
         return n * (8 + 8 + 8ull * kTrials + 4 + 1 + 4 + 4 + 4 + 4 + 8) + (D + 1) * 8 +
@@ -96,6 +110,7 @@ struct Server {
                     admit.push_back(r);
                 }
             }
+            const double t_adm = now_seconds();
             for (ServerRequest *r : admit) {
                 r->graph.reset(new DeviceGraph());
                 r->graph->host = std::move(r->host);
@@ -115,6 +130,7 @@ struct Server {
                 std::lock_guard<std::mutex> lk(mu);
                 active.push_back(r);
             }
+            if (!admit.empty()) account(0, t_adm);
             if (active.empty()) continue;
             max_active = std::max<uint64_t>(max_active, active.size());
             jobs.clear();
@@ -129,12 +145,16 @@ struct Server {
                 jobs.push_back(r->job.get());
                 reqs.push_back(q);
                 owners.push_back(r);
-                samples += q.count;
             }
             if (jobs.empty()) continue;
+            // short rounds: a small request does not wait behind a large one
+            eng.fair_share(jobs, reqs, kServeRoundMs);
             std::vector<uint64_t> nrec;
+            const double t_round = now_seconds();
             int rc = eng.round(jobs, reqs, nrec);
+            account(1, t_round);
             rounds++;
+            for (const JobRequest &q : reqs) samples += q.count;
             if (rc != SILVAN_OK) {
                 // a device error poisons every job in the round
                 for (ServerRequest *r : owners) finish(r, rc);
@@ -143,8 +163,10 @@ struct Server {
             const uint32_t la = eng.free_samples() / std::max<size_t>(1, owners.size());
             for (size_t i = 0; i < owners.size(); i++) {
                 ServerRequest *r = owners[i];
+                const double t_commit = now_seconds();
                 int e = r->job->on_drawn(reqs[i], nrec[i]);
                 r->job->set_lookahead(la);
+                account(2, t_commit);
                 if (e != SILVAN_OK) finish(r, e);
                 else if (r->job->done()) finish(r, SILVAN_OK);
             }
@@ -153,6 +175,12 @@ struct Server {
 
     // Completes a request: keeps its outputs on the host, frees its device state.
     void finish(ServerRequest *r, int rc) {
+        const double t_fin = now_seconds();
+        struct Acc {
+            Server *s;
+            double t;
+            ~Acc() { s->account(3, t); }
+        } acc{this, t_fin};
         if (rc == SILVAN_OK && r->job) {
             r->job->finish(&r->result);
             r->estimates.resize(r->graph->n);
@@ -308,6 +336,14 @@ int server_stats(Server *s, silvan_server_stats_t *st) {
     st->bytes_in_use = s->used;
     st->budget = s->budget;
     st->slots = s->eng.slots();
+    st->admit_s = s->t_acc[0];
+    st->round_s = s->t_acc[1];
+    st->commit_s = s->t_acc[2];
+    st->finish_s = s->t_acc[3];
+    st->admit_max_s = s->t_max[0];
+    st->round_max_s = s->t_max[1];
+    st->commit_max_s = s->t_max[2];
+    st->finish_max_s = s->t_max[3];
     return SILVAN_OK;
 }
 
