@@ -312,9 +312,14 @@ __device__ void expand_level(const SegDesc &A, SamplerSmem<BLOCK> &s, NodeRec *r
                     code[k] = 3;  // valid, state not read yet
                 }
             }
-            uint32_t sty[kItems];
+            // the neighbour's state, and its row (needed only if it joins; loaded
+            // now so that the join does not wait for it)
+            uint32_t sty[kItems], dg[kItems];
 #pragma unroll
-            for (int k = 0; k < kItems; k++) sty[k] = code[k] ? __ldcg(&rec[ys[k]].st) : 0u;
+            for (int k = 0; k < kItems; k++) {
+                sty[k] = code[k] ? __ldcg(&rec[ys[k]].st) : 0u;
+                dg[k] = code[k] ? __ldg(&off[ys[k] + 1]) - __ldg(&off[ys[k]]) : 0u;
+            }
 #pragma unroll
             for (int k = 0; k < kItems; k++) {
                 if (!code[k]) continue;
@@ -343,7 +348,7 @@ __device__ void expand_level(const SegDesc &A, SamplerSmem<BLOCK> &s, NodeRec *r
                 fv[k] = code[k] == 1
                             ? __ldcg(reinterpret_cast<const unsigned long long *>(&rec[ys[k]].first))
                             : 0ull;
-            uint32_t rn[kItems], rm[kItems], dg[kItems];
+            uint32_t rn[kItems], rm[kItems];
 #pragma unroll
             for (int k = 0; k < kItems; k++) {
                 const uint32_t it = t0 + (uint32_t)(k * BLOCK) + threadIdx.x;
@@ -351,12 +356,6 @@ __device__ void expand_level(const SegDesc &A, SamplerSmem<BLOCK> &s, NodeRec *r
                     hits_local++;
                     if ((uint32_t)(fv[k] >> 32) != gbase + it) code[k] = 0;
                 }
-            }
-            // degrees of the joining nodes, loaded before the ordered scan
-#pragma unroll
-            for (int k = 0; k < kItems; k++) {
-                dg[k] = 0;
-                if (code[k] == 1) dg[k] = __ldg(&off[ys[k] + 1]) - __ldg(&off[ys[k]]);
             }
 #pragma unroll
             for (int k = 0; k < kItems; k++) {
