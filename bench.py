@@ -36,7 +36,6 @@ import ctypes as C
 import json
 import os
 import statistics
-import subprocess
 import sys
 import threading
 import time
@@ -111,58 +110,60 @@ def job_kwargs(cfg):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clocks and throttle reasons sampled during the timed region: NVML
+    polled every 5 ms from a thread (reads only), so that even a timed region
+    of a few milliseconds gets samples."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = {"hw_slowdown": 0x8, "hw_thermal_slowdown": 0x40, "sw_thermal_slowdown": 0x20,
+               "sw_power_cap": 0x4}
 
     def __init__(self, gpu_index):
         self.gpu = gpu_index
-        self.proc = None
-        self.lines = []
+        self.samples = []
+        self.max_mhz = None
+        self.stop = threading.Event()
+        self.t = None
 
     def __enter__(self):
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
-                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
+            import pynvml
+            pynvml.nvmlInit()
+            dev = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+            idx = int(dev.split(",")[self.gpu]) if dev and dev.split(",")[0].isdigit() else self.gpu
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(idx)
+            self.nv = pynvml
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+            self.t = threading.Thread(target=self._poll, daemon=True)
             self.t.start()
         except Exception:
-            self.proc = None
+            self.t = None
         return self
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
+    def _poll(self):
+        nv = self.nv
+        while not self.stop.is_set():
+            try:
+                mhz = nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)
+                reasons = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                self.samples.append((mhz, reasons))
+            except Exception:
+                pass
+            self.stop.wait(0.005)
 
     def __exit__(self, *a):
-        if self.proc:
-            self.proc.terminate()
-            try:
-                self.proc.wait(timeout=5)
-            except Exception:
-                self.proc.kill()
+        self.stop.set()
+        if self.t:
+            self.t.join(timeout=2)
 
     def summary(self):
-        sm, mx, reasons = [], 0, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            f = [x.strip() for x in ln.split(",")]
-            if len(f) < 9:
-                continue
-            try:
-                sm.append(float(f[1]))
-                mx = max(mx, float(f[2]))
-            except ValueError:
-                continue
-            for nm, v in zip(names, f[5:9]):
-                if v.lower() == "active":
+        sm = [m for m, _ in self.samples]
+        reasons = set()
+        for _, r in self.samples:
+            for nm, bit in self.REASONS.items():
+                if r & bit:
                     reasons.add(nm)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx or None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(reasons), "samples": len(sm), "source": "NVML, 5 ms"}
 
 
 def refbench_lib():
@@ -632,13 +633,16 @@ def main():
                   for r in results)
         t_samp = sum(r["time_sampling_s"] for r in results)
         achieved = alg / t_samp / 1e9 if t_samp > 0 else 0.0
+        # DRAM bytes per launch: bytes per sample from an ncu capture of the
+        # same kernel on this workload (profiles/), times samples per launch
         traffic = None
         tp = os.path.join(ROOT, "profiles", "sampler_traffic.json")
         if os.path.exists(tp):
             with open(tp) as f:
                 tj = json.load(f)
-            if tj.get("workload") == cfg["workload"]:
-                traffic = tj.get("bytes_per_launch")
+            launches_all = sum(r["sampler_launches"] for r in results)
+            if tj.get("workload") == cfg["workload"] and launches_all:
+                traffic = tj["dram_bytes_per_sample"] * samples / launches_all
         cpu = None
         if not args.no_cpu_baseline:
             lib = refbench_lib()
