@@ -78,7 +78,18 @@ typedef struct {
     uint32_t threads;    /* divisor of union_sample (0 = 1, parity mode)    */
     uint32_t block;      /* threads per sampler slot: 0 = autotuned per graph
                             and round, else 128, 256, 512 or 1024            */
+    uint32_t backtrack;  /* SILVAN_BACKTRACK_*                               */
+    uint32_t reserved;
 } silvan_params_t;
+
+/* Predecessor choice of the random backtrack.  REFERENCE is the rule of
+ * silvan/src/Sp_sampler.cpp:241-265 as written (its running counter adds
+ * n_paths of the sample's endpoint, 1, per predecessor: bit-exact parity).
+ * SIGMA_WEIGHTED adds n_paths of each predecessor instead (in 64 bits), so
+ * every shortest path is equally likely; it is an option of this library and
+ * outside the reference's parity. */
+#define SILVAN_BACKTRACK_REFERENCE 0
+#define SILVAN_BACKTRACK_SIGMA_WEIGHTED 1
 
 /* Fills p with the reference defaults. */
 void silvan_params_default(silvan_params_t *p);

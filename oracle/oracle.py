@@ -139,7 +139,7 @@ class Port:
         lib.orc_run.restype = C.c_int
         lib.orc_run.argtypes = [C.c_void_p, C.c_uint32, C.c_double, C.c_double, C.c_uint32,
                                 C.c_double, C.c_int, C.c_double, C.c_int, C.c_uint64,
-                                C.c_uint32, C.c_void_p]
+                                C.c_uint32, C.c_int, C.c_void_p]
         lib.orc_result_size.restype = C.c_uint64
         for f in ("orc_run_arrays", "orc_run_ranking", "orc_run_sp_lengths", "orc_run_partitions"):
             getattr(lib, f).restype = None
@@ -179,11 +179,11 @@ class PortGraph:
         return out
 
     def run(self, diameter, eps, delta, k=0, alpha=2.3, alpha_given=False, a=2.0, mhat=True,
-            seed=42, threads=1):
+            seed=42, threads=1, weighted=False):
         res = RunResult()
         lib = self.port.lib
         lib.orc_run(self.h, diameter, eps, delta, k, alpha, int(alpha_given), a, int(mhat), seed,
-                    threads, C.byref(res))
+                    threads, int(weighted), C.byref(res))
         n = self.n
         out = {f: getattr(res, f) for f, _ in RunResult._fields_}
         approx = np.zeros(n, np.float64)

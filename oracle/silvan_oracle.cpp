@@ -70,18 +70,27 @@ enum { UNVISITED = 0, SIDE_U = 1, SIDE_V = 2 };
 // (silvan/src/Sp_sampler.cpp:241-265).  The running counter adds
 // n_paths[v] of the sample's endpoint v, which is always 1, so the chosen
 // predecessor is pred[start][min(r, |pred|-1)] with r = draw mod sigma(start).
+// With `weighted` the counter adds n_paths[w] of the predecessor itself (in
+// 64 bits), the rule that picks each shortest path with equal probability;
+// it is an option of this library, not the reference's behaviour.
 void backtrack(const Scratch &s, Stream &rng, uint32_t u, uint32_t v, uint32_t start,
-               std::vector<uint32_t> &path) {
+               std::vector<uint32_t> &path, bool weighted) {
     while (start != u && start != v) {
         path.push_back(start);
         uint32_t r = (uint32_t)rng.get_max(s.sigma[start]);
         const std::vector<uint32_t> &p = s.pred[start];
         uint32_t w = 0;
         uint32_t acc = 0;
+        uint64_t acc64 = 0;
         for (uint32_t t = 0; t < p.size(); t++) {
             w = p[t];
-            acc += (uint32_t)s.sigma[v];
-            if (acc > r) break;
+            if (weighted) {
+                acc64 += s.sigma[w];
+                if (acc64 > r) break;
+            } else {
+                acc += (uint32_t)s.sigma[v];
+                if (acc > r) break;
+            }
         }
         start = w;
     }
@@ -89,7 +98,7 @@ void backtrack(const Scratch &s, Stream &rng, uint32_t u, uint32_t v, uint32_t s
 
 // silvan/src/Sp_sampler.cpp:41-238 (random_path).
 void sample_one(const OGraph &g, Scratch &s, uint64_t seed, uint32_t index, double alpha,
-                SampleOut &out) {
+                SampleOut &out, bool weighted = false) {
     Stream rng{seed, index, 0};
     out = SampleOut();
     const uint32_t n = g.n;
@@ -197,8 +206,8 @@ void sample_one(const OGraph &g, Scratch &s, uint64_t seed, uint32_t index, doub
         for (auto &p : meet) {
             cum += s.sigma[p.first] * s.sigma[p.second];
             if (cum > r) {
-                backtrack(s, rng, u, v, p.first, path);
-                backtrack(s, rng, u, v, p.second, path);
+                backtrack(s, rng, u, v, p.first, path, weighted);
+                backtrack(s, rng, u, v, p.second, path, weighted);
                 break;
             }
         }
@@ -245,6 +254,7 @@ struct Params {
     int mhat;
     uint64_t seed;
     uint32_t threads;  // union_sample divisor (1 in parity mode)
+    int weighted;      // sigma-weighted backtrack (an option, not the reference)
 };
 
 struct Result {
@@ -308,7 +318,7 @@ struct Run {
     void one_round() {
         SampleOut s;
         uint32_t idx = next_index++;
-        sample_one(g, scratch, p.seed, idx, alpha, s);
+        sample_one(g, scratch, p.seed, idx, alpha, s, p.weighted != 0);
         if (s.zero_mod) zero_mod = true;
         n_pairs++;
         vis_edges += s.vis_edges;
@@ -804,9 +814,10 @@ int64_t orc_replay(void *gp, uint64_t seed, uint32_t first, uint32_t count, doub
 // Full estimator run in parity mode.  res must point to an OrcResult
 // (layout of `Result` above).
 int orc_run(void *gp, uint32_t diameter, double eps, double delta, uint32_t k, double alpha,
-            int alpha_given, double a, int mhat, uint64_t seed, uint32_t threads, void *res) {
+            int alpha_given, double a, int mhat, uint64_t seed, uint32_t threads, int weighted,
+            void *res) {
     delete g_run;
-    Params p{eps, delta, k, alpha, alpha_given, a, mhat, seed, threads ? threads : 1};
+    Params p{eps, delta, k, alpha, alpha_given, a, mhat, seed, threads ? threads : 1, weighted};
     g_run = new Run(*(OGraph *)gp, p, diameter);
     g_run->run(*(Result *)res);
     return 0;

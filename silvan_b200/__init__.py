@@ -23,6 +23,7 @@ OK = 0
 E_BADARG, E_IO, E_PARSE, E_OOM, E_CUDA = -1, -2, -3, -4, -5
 E_OVERFLOW, E_NP_CAP, E_TIMEOUT, E_CAPACITY, E_STATE, E_NOGPU = -6, -7, -8, -9, -10, -11
 FORM_PLAIN, FORM_BATCHED = 0, 1
+BACKTRACK_REFERENCE, BACKTRACK_SIGMA_WEIGHTED = 0, 1
 TRIALS = 25
 
 # Every function declared in include/silvan.h.
@@ -58,7 +59,8 @@ class Params(C.Structure):
                 ("m_hat", C.c_int32), ("alpha", C.c_double), ("alpha_given", C.c_int32),
                 ("form", C.c_int32), ("a", C.c_double), ("seed", C.c_uint64),
                 ("verbose", C.c_double), ("np_cap", C.c_uint32), ("slots", C.c_uint32),
-                ("threads", C.c_uint32), ("block", C.c_uint32)]
+                ("threads", C.c_uint32), ("block", C.c_uint32),
+                ("backtrack", C.c_uint32), ("reserved", C.c_uint32)]
 
 
 class Result(C.Structure):
@@ -363,7 +365,7 @@ class Probabilistic:
 
     def __init__(self, graph: Graph, eps, delta, k=0, alpha=2.3, alpha_given=False, a=2.0,
                  m_hat=True, seed=42, form="batched", verbose=0.0, np_cap=0, slots=0,
-                 threads=1, block=0):
+                 threads=1, block=0, backtrack="reference"):
         lib = load()
         p = Params()
         lib.silvan_params_default(C.byref(p))
@@ -372,6 +374,8 @@ class Probabilistic:
         p.m_hat, p.seed, p.verbose = int(m_hat), seed, verbose
         p.form = FORM_PLAIN if form == "plain" else FORM_BATCHED
         p.np_cap, p.slots, p.threads, p.block = np_cap, slots, threads, block
+        p.backtrack = {"reference": BACKTRACK_REFERENCE,
+                       "sigma": BACKTRACK_SIGMA_WEIGHTED}[backtrack]
         self.graph = graph
         self.params = p
         h = C.c_void_p()

@@ -559,6 +559,7 @@ int Engine::round(const std::vector<Job *> &jobs, const std::vector<JobRequest> 
         S.seed = job->params().seed;
         S.alpha = job->alpha();
         S.np_cap = job->params().np_cap;
+        S.weighted = job->params().backtrack == SILVAN_BACKTRACK_SIGMA_WEIGHTED ? 1 : 0;
         S.first_sample = r.first_global;
         S.count = r.count;
         S.base = base;
@@ -847,6 +848,11 @@ int Job::init() {
     if (p_.block != 0 && p_.block != 128 && p_.block != 256 && p_.block != 512 &&
         p_.block != 1024) {
         set_error("block must be 0 (autotuned), 128, 256, 512 or 1024");
+        return SILVAN_E_BADARG;
+    }
+    if (p_.backtrack != SILVAN_BACKTRACK_REFERENCE &&
+        p_.backtrack != SILVAN_BACKTRACK_SIGMA_WEIGHTED) {
+        set_error("backtrack must be SILVAN_BACKTRACK_REFERENCE or SILVAN_BACKTRACK_SIGMA_WEIGHTED");
         return SILVAN_E_BADARG;
     }
     if (p_.np_cap == 0) p_.np_cap = 1u << 24;

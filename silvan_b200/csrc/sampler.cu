@@ -221,6 +221,47 @@ __device__ uint32_t middle_pred(const SegDesc &A, const Smem &s, const NodeRec *
     return bx;
 }
 
+// Sigma-weighted predecessor of node a (cnt >= 2): the first predecessor in
+// queue order whose running sum of sigma exceeds r, r = draw mod sigma(a).
+// The predecessors are the reverse-direction neighbours on the previous level
+// of a's side; their queue order is the order of their own first-hit keys, so
+// they are taken one at a time by increasing key.
+__device__ uint32_t weighted_pred(const SegDesc &A, const NodeRec *rec, uint32_t a,
+                                  uint32_t st_a, uint32_t cnt, uint32_t r, int32_t &status) {
+    const uint32_t side = st_side(st_a);
+    const uint32_t want = st_make(side, st_dist(st_a) - 1u);
+    const uint32_t *roff = side == kSideU ? A.in_off : A.out_off;
+    const uint32_t *radj = side == kSideU ? A.in_adj : A.out_adj;
+    const uint32_t rb = roff[a], re = roff[a + 1];
+    unsigned long long acc = 0, prev = 0;
+    bool have_prev = false;
+    uint32_t last = a;
+    for (uint32_t i = 0; i < cnt; i++) {
+        unsigned long long best = ~0ull, bs = 0;
+        uint32_t bx = a;
+        for (uint32_t k = rb; k < re; k++) {
+            const uint32_t x = radj[k];
+            if (__ldcg(&rec[x].st) != want) continue;
+            const unsigned long long kx = __ldcg(&rec[x].first) >> 32;
+            if ((!have_prev || kx > prev) && kx < best) {
+                best = kx;
+                bx = x;
+                bs = __ldcg(&rec[x].sigma);
+            }
+        }
+        if (bx == a) {
+            status = SILVAN_E_STATE;
+            return a;
+        }
+        acc += bs;
+        last = bx;
+        if (acc > (unsigned long long)r) return bx;
+        prev = best;
+        have_prev = true;
+    }
+    return last;
+}
+
 // Expands one BFS level of `side` (silvan/src/Sp_sampler.cpp:89-143).
 //
 // The level is latency-bound on deep, narrow searches (a grid's ~200 levels
@@ -706,7 +747,14 @@ __global__ void __launch_bounds__(BLOCK, Shape<BLOCK>::kMinBlocks) sampler_kerne
                             rr = mod_u64(rr, sg);
                             const uint32_t c = r0.y;
                             const uint32_t t = min(rr, c - 1u);
-                            if (t == 0) {
+                            if (A.weighted && c > 1u) {
+                                int32_t e = 0;
+                                a = weighted_pred(A, rec, a, sta, c, rr, e);
+                                if (e) {
+                                    s.status = e;
+                                    break;
+                                }
+                            } else if (t == 0) {
                                 a = r1.x;  // low word of first: the joining predecessor
                             } else if (t == c - 1u) {
                                 a = r1.z;  // low word of last

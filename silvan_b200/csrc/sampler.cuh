@@ -29,6 +29,7 @@ struct SegDesc {
     uint32_t first_sample;  // global index of the segment's sample 0
     uint32_t count;
     uint32_t base;          // work index of the segment's sample 0 (prefix over segments)
+    int32_t weighted;       // sigma-weighted backtrack (SILVAN_BACKTRACK_SIGMA_WEIGHTED)
     // per-sample outputs, segment-local index
     int32_t *out_pl;
     int32_t *out_np;

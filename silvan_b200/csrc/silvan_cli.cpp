@@ -9,7 +9,8 @@
 // Options beyond the reference's (long options, so that the reference's
 // short-option set is unchanged): --plain (one launch sequence per 11-sample
 // block), --seed N (job seed), --np-cap N (paths per sample), --slots N,
-// --block N (threads per sampler slot; default autotuned).
+// --block N (threads per sampler slot; default autotuned), --sigma-weighted
+// (the path-count-weighted backtrack instead of the reference's rule).
 #include <cerrno>
 #include <climits>
 #include <cstdio>
@@ -40,6 +41,7 @@ bool m_hat = true;
 bool plain = false;
 uint64_t seed = 42;
 uint32_t np_cap = 0, slots = 0, block = 0;
+bool sigma_weighted = false;
 
 // silvan/main.cpp:51-68
 void usage(const char *b) {
@@ -68,6 +70,8 @@ void usage(const char *b) {
     std::cerr << "\t--seed N, --np-cap N, --slots N, --block N: job seed, paths per sample, "
                  "sampler slots, threads per slot"
               << std::endl;
+    std::cerr << "\t--sigma-weighted: pick predecessors by path count (not the reference's rule)"
+              << std::endl;
 }
 
 // silvan/main.cpp:74-153: 0 ok, 1 error, 2 help
@@ -77,6 +81,7 @@ int parse(int argc, char **argv) {
                                        {"np-cap", required_argument, nullptr, 3},
                                        {"slots", required_argument, nullptr, 4},
                                        {"block", required_argument, nullptr, 5},
+                                       {"sigma-weighted", no_argument, nullptr, 6},
                                        {nullptr, 0, nullptr, 0}};
     int opt;
     while ((opt = getopt_long(argc, argv, "dhmk:o:s:a:v:", longopts, nullptr)) != -1) {
@@ -122,6 +127,7 @@ int parse(int argc, char **argv) {
             case 3: np_cap = (uint32_t)std::strtoul(optarg, nullptr, 10); break;
             case 4: slots = (uint32_t)std::strtoul(optarg, nullptr, 10); break;
             case 5: block = (uint32_t)std::strtoul(optarg, nullptr, 10); break;
+            case 6: sigma_weighted = true; break;
             default: break;
         }
     }
@@ -192,6 +198,7 @@ int main(int argc, char **argv) {
     p.np_cap = np_cap;
     p.slots = slots;
     p.block = block;
+    p.backtrack = sigma_weighted ? SILVAN_BACKTRACK_SIGMA_WEIGHTED : SILVAN_BACKTRACK_REFERENCE;
     silvan_job_t j = nullptr;
     rc = silvan_job_create(g, &p, &j);
     if (rc != SILVAN_OK) {

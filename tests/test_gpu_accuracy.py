@@ -41,3 +41,20 @@ def test_oracle_estimates_within_eps(port, ba10k):
         o = pg.run(csr.diameter, EPS, DELTA, seed=2000 + seed)
         errs.append(float(np.abs(o["approx"] / o["num_samples"] - bc).max()))
     assert max(errs) <= EPS, errs
+
+
+@pytest.mark.gpu
+def test_sigma_weighted_backtrack_within_eps_on_a_lattice(sb, port):
+    """On a lattice the reference's backtrack rule is biased (see
+    test_oracle.py); the sigma-weighted option keeps every estimate within
+    eps of exact betweenness."""
+    hg = sb.HostGraph.from_pairs(sb.grid(16, 0.0, 0.0, 1), False)
+    csr = hg.csr()
+    bc = port.graph(csr.n, False, csr.out_off, csr.out_adj, csr.in_off, csr.in_adj,
+                    csr.cc).brandes()
+    g = sb.Graph.from_host(hg)
+    for seed in range(5):
+        job = sb.Probabilistic(g, EPS, DELTA, seed=seed, alpha=0.0, alpha_given=True,
+                               backtrack="sigma")
+        job.run()
+        assert np.abs(job.get_centrality() - bc).max() <= EPS

@@ -20,9 +20,11 @@ def run_pair(sb, port, small_graphs, name, eps, delta, **kw):
     hg, csr, _ = small_graphs[name]
     job = sb.Probabilistic(sb.Graph.from_host(hg), eps, delta, **kw)
     res = job.run()
-    okw = {k: v for k, v in kw.items() if k not in ("block", "slots", "form")}
+    okw = {k: v for k, v in kw.items() if k not in ("block", "slots", "form", "backtrack")}
     if "m_hat" in okw:
         okw["mhat"] = okw.pop("m_hat")
+    if kw.get("backtrack") == "sigma":
+        okw["weighted"] = True
     o = port_graph(port, csr).run(csr.diameter, eps, delta, **okw)
     return job, res, o
 
@@ -86,3 +88,18 @@ def test_plain_and_batched_topk_agree(sb, small_graphs):
     assert out[0][0] == out[1][0]
     np.testing.assert_array_equal(out[0][1][0], out[1][1][0])
     np.testing.assert_array_equal(out[0][2], out[1][2])
+
+
+@pytest.mark.parametrize("name,extra", [
+    ("ba2k", {}),
+    ("rmat11d", {"block": 128}),
+    ("grid40", {"alpha": 0.0, "alpha_given": True}),
+    ("grid40", {"k": 10, "alpha": 0.0, "alpha_given": True}),
+])
+def test_sigma_weighted_backtrack_matches_oracle(sb, port, small_graphs, name, extra):
+    """The sigma-weighted backtrack option (not the reference's rule) against
+    the oracle's restatement of the same rule."""
+    eps = 0.1 if extra.get("k") else 0.03
+    job, res, o = run_pair(sb, port, small_graphs, name, eps, 0.1, seed=17, backtrack="sigma",
+                           **extra)
+    assert_same_run(job, res, o)

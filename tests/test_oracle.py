@@ -171,3 +171,21 @@ def test_brandes_matches_pair_enumeration(sb, port, directed):
     p3 = sb.HostGraph.from_pairs(np.array([[0, 1], [1, 2]], np.uint32), False).csr()
     b3 = port.graph(p3.n, False, p3.out_off, p3.out_adj, p3.in_off, p3.in_adj, p3.cc).brandes()
     np.testing.assert_allclose(b3, [0, 1 / 3, 0])
+
+
+def test_weighted_backtrack_restores_the_guarantee_on_a_lattice(sb, port):
+    """On a lattice most pairs have many shortest paths.  The reference's
+    backtrack (Sp_sampler.cpp:254-260 adds n_paths of the endpoint, 1, per
+    predecessor) does not pick them uniformly, and its estimates miss exact
+    betweenness by more than eps; the sigma-weighted option does not."""
+    hg = sb.HostGraph.from_pairs(sb.grid(8, 0.0, 0.0, 1), False)
+    csr = hg.csr()
+    pg = port.graph(csr.n, False, csr.out_off, csr.out_adj, csr.in_off, csr.in_adj, csr.cc)
+    bc = pg.brandes()
+    eps = 0.01
+    for seed in range(3):
+        kw = dict(seed=seed, alpha=0.0, alpha_given=True)
+        ref = pg.run(csr.diameter, eps, 0.05, **kw)
+        wtd = pg.run(csr.diameter, eps, 0.05, weighted=True, **kw)
+        assert np.abs(ref["approx"] / ref["num_samples"] - bc).max() > eps
+        assert np.abs(wtd["approx"] / wtd["num_samples"] - bc).max() <= eps
