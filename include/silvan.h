@@ -133,8 +133,10 @@ typedef struct {
 /* ---- graphs (reference: Graph, silvan/src/Graph.cpp) ------------------- */
 
 /* Graph(filename, directed) (silvan/src/Graph.cpp:37-90) followed by
- * compute_cc + estimate_diameter (silvan/src/Graph.cpp:109-316), then the
- * CSR and component ids are copied to the device. */
+ * compute_cc + estimate_diameter (silvan/src/Graph.cpp:109-316).  The edge
+ * list is parsed and the CSR built on the device, with the reference
+ * loader's line semantics (the same graph as silvan_host_graph_load); the
+ * components and the diameter bound are computed on a host copy. */
 int silvan_graph_load(const char *path, int directed, silvan_graph_t *out);
 
 /* Same, from host CSR arrays (rows ascending, unique).  in_off/in_adj are

@@ -6,6 +6,7 @@
 #include <vector>
 
 #include "engine.h"
+#include "ingest.h"
 #include "gen.h"
 #include "server.h"
 #include "silvan.h"
@@ -104,14 +105,17 @@ int silvan_graph_load(const char *path, int directed, silvan_graph_t *out) {
     if (rc) return rc;
     silvan_graph_s *G = new (std::nothrow) silvan_graph_s();
     if (!G) return SILVAN_E_OOM;
+    // parsed and built on the device (ingest.cu); the host loader
+    // (silvan_host_graph_load) gives the same graph
     std::string err;
-    rc = load_edge_list(path, directed != 0, G->g.host, err);
+    rc = device_ingest(path, directed != 0, G->g, err);
     if (rc != SILVAN_OK) {
-        set_error(err);
+        if (!err.empty()) set_error(err);
         delete G;
         return rc;
     }
-    return finish_graph(G, false, out);
+    *out = G;
+    return SILVAN_OK;
 }
 
 int silvan_graph_upload(uint32_t n, int directed, const uint64_t *out_off,

@@ -160,6 +160,19 @@ void hfree(T *&p) {
 }
 }  // namespace
 
+int device_alloc(void **p, size_t bytes) {
+    cudaError_t e;
+    *p = block_cache().alloc(bytes ? bytes : 1, false, &e);
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        set_error(std::string("device allocation failed: ") + cudaGetErrorString(e));
+        return SILVAN_E_OOM;
+    }
+    return SILVAN_OK;
+}
+
+void device_free(void *p) { block_cache().free(p); }
+
 void set_error(const std::string &msg) { g_err = msg; }
 const char *last_error_cstr() { return g_err.c_str(); }
 
@@ -223,6 +236,16 @@ int DeviceGraph::upload() {
         d_in_off = d_out_off;
         d_in_adj = d_out_adj;
     }
+    RK(dmalloc(&d_cc, n));
+    CK(cudaMemcpy(d_cc, cc.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice));
+    return SILVAN_OK;
+}
+
+int DeviceGraph::finish_from_host_copy() {
+    const double t0 = now_seconds();
+    ncomp = compute_scc(host, cc);
+    diameter = estimate_diameter(host, cc, ncomp);
+    diameter_seconds = now_seconds() - t0;
     RK(dmalloc(&d_cc, n));
     CK(cudaMemcpy(d_cc, cc.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice));
     return SILVAN_OK;

@@ -28,6 +28,12 @@ void set_error(const std::string &msg);
 int cuda_status(cudaError_t e, const char *what);
 double now_seconds();
 
+// Device memory from the library's caching allocator: freed blocks are kept
+// per device and size class and handed out again.  Every device buffer that a
+// DeviceGraph, Engine or Job frees must come from here.
+int device_alloc(void **p, size_t bytes);
+void device_free(void *p);
+
 struct DeviceGraph {
     // metadata (always set once uploaded)
     uint32_t n = 0;
@@ -57,6 +63,9 @@ struct DeviceGraph {
     int upload_raw(uint32_t n, bool directed, const uint64_t *out_off, const uint32_t *out_adj,
                    const uint64_t *in_off, const uint32_t *in_adj, const uint32_t *cc);
     uint64_t device_bytes() const;
+    // Components and diameter bound on the host copy, then the component
+    // ids to the device (after a device ingest filled d_* and `host`).
+    int finish_from_host_copy();
     ~DeviceGraph();
 };
 
