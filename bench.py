@@ -23,10 +23,11 @@ reference reports as "Total time".  time-to-(eps,delta) is reported beside it.
 Other workloads (--config): ba10k (Barabasi-Albert n = 10^4), grid2048 (top-10
 on a 2048 x 2048 lattice with shortcuts), multigraph64 (64 graphs of uneven
 size in one batched run), serve (a Poisson stream of requests on fresh R-MAT
-graphs: p50/p99 latency and paths/s under continuous batching).
+graphs: p50/p99 latency and paths/s under continuous batching), ingest
+(loading the R-MAT 20 edge list: device parse and CSR build).
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                       [--config rmat20|ba10k|grid2048|multigraph64|serve]
+                       [--config rmat20|ba10k|grid2048|multigraph64|serve|ingest]
                        [--form batched|plain] [--block 0|128|256|512|1024]
 """
 from __future__ import annotations
@@ -65,6 +66,10 @@ CONFIGS = {
     # top-10 requests take their relative eps as 10 x that draw: at relative
     # eps 0.01 one scale-20 top-10 request alone needs over 4 * 10^7 samples)
     "serve": dict(kind="serve", workload="rmat_scale10_20_poisson_stream", delta=0.05),
+    # Graph(filename) on the R-MAT 20 edge list: device parse + CSR build
+    # (silvan_graph_load) against the host loader and the reference's own
+    "ingest": dict(kind="ingest", workload="rmat20_directed_ef16_seed2_edge_list", scale=20,
+                   edge_factor=16, seed=2, directed=True),
 }
 
 
@@ -243,6 +248,10 @@ def run_reference_arm(args, cfg):
         print(json.dumps({"impl": "reference", "unavailable":
                           "the reference has no request server; the serve line carries its "
                           "CPU baseline"}))
+        return 0
+    if cfg["kind"] == "ingest":
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "the ingest line carries the reference loader's time"}))
         return 0
     threads = os.cpu_count() or 1
     holder = {}
@@ -520,6 +529,76 @@ def run_serve(args, cfg):
     return 0
 
 
+def run_ingest(args, cfg):
+    """Loading the benchmark graph from its 'u v' text file: the device
+    ingest (parse and CSR on the GPU, components and diameter bound on the
+    host copy), this library's host loader, and the reference's own loader
+    (std::set insertion, silvan/src/Graph.cpp:37-90) once."""
+    rank, _, local = dist_env()
+    if rank != 0:
+        return 0
+    import tempfile
+
+    import torch
+    import silvan_b200 as sb
+    torch.cuda.set_device(local)
+    fd, path = tempfile.mkstemp(suffix=".txt")
+    os.close(fd)
+    try:
+        sb.write_edge_list(path, sb.rmat(cfg["scale"], cfg["edge_factor"], cfg["seed"],
+                                         cfg["directed"]))
+        size = os.path.getsize(path)
+        for _ in range(args.warmup):
+            del_g = sb.Graph.load(path, cfg["directed"])
+            del del_g
+        dev, host = [], []
+        with ClockSampler(local) as clk:
+            for _ in range(args.steps):
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                g = sb.Graph.load(path, cfg["directed"])
+                torch.cuda.synchronize()
+                dev.append(time.perf_counter() - t0)
+                del g
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            h = sb.HostGraph.load(path, cfg["directed"])
+            host.append(time.perf_counter() - t0)
+            edges = int(h.info().m)
+            del h
+        ref_s = None
+        if not args.no_cpu_baseline:
+            try:
+                from oracle.oracle import Ref, ref_available
+                if ref_available():
+                    t0 = time.perf_counter()
+                    rg = Ref().graph(path, cfg["directed"])
+                    ref_s = time.perf_counter() - t0
+                    del rg
+            except Exception:
+                ref_s = None
+    finally:
+        os.unlink(path)
+    t = sum(dev) / len(dev)
+    print(json.dumps({
+        "metric": "edge-list ingest", "value": size / t / 1e6, "unit": "MB/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * t,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8/u32",
+        "data": "synthetic",
+        "config": {"workload": cfg["workload"], "file_bytes": size, "edges": edges,
+                   "includes": "file read, H2D, parse, CSR, read-back, host components and "
+                               "diameter bound"},
+        "host_loader_s": sum(host) / len(host),
+        "reference_loader_s": ref_s,
+        "cpu_baseline": {"value": size / ref_s / 1e6, "unit": "MB/s", "cores": 1,
+                         "kind": "reference",
+                         "sample": "one Graph(filename, directed) of the reference"}
+        if ref_s else None,
+        "clocks": clk.summary(),
+    }))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -547,6 +626,8 @@ def main():
         return run_multi(args, cfg)
     if cfg["kind"] == "serve":
         return run_serve(args, cfg)
+    if cfg["kind"] == "ingest":
+        return run_ingest(args, cfg)
 
     import numpy as np
     import torch
@@ -667,6 +748,7 @@ def main():
                        / args.steps},
             "time_to_guarantee_ms": 1000 * t_max / args.steps,
             "samples_per_step": samples_all / max(1, world) / args.steps,
+            "samples_drawn_per_step": sum(r["samples_drawn"] for r in results) / args.steps,
             "backtracked_paths_per_step": sum(r["backtracked_paths"] for r in results) /
                                           args.steps,
             "e2e": {"value": e2e_s_all / e2e_t_max if e2e_t_max > 0 else None,

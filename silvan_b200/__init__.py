@@ -79,7 +79,8 @@ class Result(C.Structure):
                 ("time_sampling_s", C.c_double), ("time_apply_s", C.c_double),
                 ("time_device_s", C.c_double), ("ball_nodes", C.c_uint64),
                 ("pred_entries", C.c_uint64), ("kernel_launches", C.c_uint64),
-                ("sampler_launches", C.c_uint32), ("sampler_block", C.c_uint32)]
+                ("sampler_launches", C.c_uint32), ("sampler_block", C.c_uint32),
+                ("samples_drawn", C.c_uint64)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}

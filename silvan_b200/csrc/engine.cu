@@ -580,7 +580,7 @@ int Engine::round(const std::vector<Job *> &jobs, const std::vector<JobRequest> 
         S.n = G.n;
         S.directed = G.directed ? 1 : 0;
         S.seed = job->params().seed;
-        S.alpha = job->alpha();
+        S.alpha = r.alpha;
         S.np_cap = job->params().np_cap;
         S.weighted = job->params().backtrack == SILVAN_BACKTRACK_SIGMA_WEIGHTED ? 1 : 0;
         S.first_sample = r.first_global;
@@ -646,6 +646,7 @@ int Engine::round(const std::vector<Job *> &jobs, const std::vector<JobRequest> 
             const double cta_ms = (double)h_hdr_->cycles / clock_khz_ / h_hdr_->total;
             const double tail_ms = (double)h_hdr_->max_cycles / clock_khz_;
             last_cta_ms_ = cta_ms;
+            last_tail_ms_ = tail_ms;
             last_launch_ms_ = ms;
             last_grid_ = grid;
             for (uint32_t i : idx) {
@@ -680,9 +681,13 @@ int Engine::round(const std::vector<Job *> &jobs, const std::vector<JobRequest> 
     return SILVAN_OK;
 }
 
-uint32_t Engine::free_samples() const {
-    if (last_cta_ms_ <= 0 || last_launch_ms_ <= 0) return 0;
-    const double f = last_launch_ms_ * last_grid_ / last_cta_ms_;
+uint32_t Engine::free_samples(bool tail_only) const {
+    // the samples the other slots draw while the slowest sample runs, or
+    // while the whole last launch ran (a throughput-bound launch feeds its own
+    // length back, so that estimate needs a cap from the caller)
+    const double t = tail_only ? last_tail_ms_ : last_launch_ms_;
+    if (last_cta_ms_ <= 0 || t <= 0) return 0;
+    const double f = t * last_grid_ / last_cta_ms_;
     return (uint32_t)std::min<double>(f, (double)kRoundSamples);
 }
 
@@ -1361,12 +1366,14 @@ bool Job::next_request(JobRequest &r) {
     uint64_t cnt = target_ - pass_samples_;
     if (p_.form == SILVAN_FORM_PLAIN) {
         cnt = std::min<uint64_t>(cnt, kBlock);
-    } else if (phase_ == kPass2) {
+    } else if (phase_ == kPass2 || absolute_) {
         // draw ahead of the next schedule point: samples are deterministic in
         // their index, so drawing early changes nothing but the launch count;
-        // the ones beyond the final stop are discarded
-        cnt = std::max<uint64_t>(cnt, lookahead_);
-        if (p_.m_hat) {
+        // the ones beyond the final stop are discarded.  In absolute mode the
+        // first pass has a fixed length, and the samples drawn beyond it are
+        // the second pass's first ones when the second pass keeps alpha.
+        cnt = std::max<uint64_t>(cnt, phase_ == kPass2 ? lookahead_ : lookahead_tail_);
+        if (phase_ == kPass2 && p_.m_hat) {
             // the omega cap only decreases, so the run never goes beyond it
             const uint64_t cap = (uint64_t)kBlock * (uint64_t)ceil(omega_ / kBlock);
             if (cap > pass_samples_) cnt = std::min<uint64_t>(cnt, cap - pass_samples_);
@@ -1377,6 +1384,7 @@ bool Job::next_request(JobRequest &r) {
     r.count = (uint32_t)cnt;
     r.pass = phase_ == kPass1 ? 1 : 2;
     r.track_cross = phase_ == kPass1 && !absolute_;
+    r.alpha = alpha_;
     if (base_global_ + pass_samples_ + cnt >= 0xffffffffull) return false;
     return cnt > 0;
 }
@@ -1505,27 +1513,37 @@ int Job::finish_pass1() {
 }
 
 int Job::on_drawn(const JobRequest &r, uint64_t n_records) {
-    // the drawn range is [lo, hi) in pass-local indices; commit it up to each
-    // schedule point in turn and evaluate the point (:828-845, :1060-1087)
-    const uint64_t lo = r.first_global - base_global_;
-    const uint64_t hi = lo + r.count;
-    if (lo != pass_samples_) {
+    // the drawn range is [g0, g1) in global sample indices; commit it up to
+    // each schedule point in turn and evaluate the point (:828-845,
+    // :1060-1087), across the end of pass 1 when the draw reaches into pass 2
+    const uint64_t g0 = r.first_global, g1 = g0 + r.count;
+    drawn_ += r.count;
+    if (g0 != base_global_ + pass_samples_) {
         set_error("drawn range does not continue the committed samples");
         return SILVAN_E_STATE;
     }
     const uint64_t save_apply = launches;
     CK(cudaEventRecord(ev_commit_[0], stream_));
     for (;;) {
-        const uint64_t c_hi = std::min(target_, hi);
-        if (c_hi > pass_samples_) {
-            RK(apply_range(r, (uint32_t)(pass_samples_ - lo), (uint32_t)(c_hi - lo), n_records));
-            pass_samples_ = c_hi;
+        JobRequest rc = r;
+        rc.pass = phase_ == kPass1 ? 1 : 2;
+        rc.track_cross = phase_ == kPass1 && !absolute_;
+        const uint64_t cur = base_global_ + pass_samples_;
+        const uint64_t c_hi = std::min(base_global_ + target_, g1);
+        if (c_hi > cur) {
+            RK(apply_range(rc, (uint32_t)(cur - g0), (uint32_t)(c_hi - g0), n_records));
+            pass_samples_ += c_hi - cur;
         }
         if (pass_samples_ < target_) break;  // the next point lies beyond the drawn range
         const Phase ph = phase_;
         RK(evaluate());
-        if (phase_ != ph || done()) break;    // new pass, or stopped
-        if (pass_samples_ != c_hi) break;     // pass 1 redrawn from the start
+        if (done()) break;
+        if (phase_ != ph) {
+            // pass 1 ended: the rest of the draw is pass 2's if drawn with its alpha
+            if (alpha_ != r.alpha) break;
+            continue;
+        }
+        if (base_global_ + pass_samples_ != c_hi) break;  // pass 1 redrawn from the start
     }
     CK(cudaEventRecord(ev_commit_[1], stream_));
     CK(cudaEventSynchronize(ev_commit_[1]));
@@ -1533,6 +1551,7 @@ int Job::on_drawn(const JobRequest &r, uint64_t n_records) {
         float ms = 0;
         cudaEventElapsedTime(&ms, ev_commit_[0], ev_commit_[1]);
         commit_ms_ += ms;
+        if (done()) result_.time_apply_s = commit_ms_ / 1000.0;  // the run ended in this call
     }
     return SILVAN_OK;
 }
@@ -1685,6 +1704,7 @@ int Job::evaluate() {
     res.kernel_launches = launches + (own_engine_ ? own_engine_->launches() : 0);
     res.sampler_launches = own_engine_ ? own_engine_->sampler_launches() : 0;
     res.sampler_block = own_engine_ ? own_engine_->main_block() : 0;
+    res.samples_drawn = drawn_;
     phase_ = kDone;
     return SILVAN_OK;
 }
@@ -1710,6 +1730,7 @@ int Job::run(silvan_result_t *res, FILE *sink) {
     std::vector<Job *> jobs{this};
     std::vector<JobRequest> reqs(1);
     std::vector<uint64_t> nrec;
+    set_lookahead(own_engine_->free_samples(true), own_engine_->free_samples(false));
     while (!done()) {
         if (!next_request(reqs[0])) {
             set_error("sample index space exhausted");
@@ -1721,7 +1742,7 @@ int Job::run(silvan_result_t *res, FILE *sink) {
             error_ = rc;
             return rc;
         }
-        lookahead_ = own_engine_->free_samples();
+        set_lookahead(own_engine_->free_samples(true), own_engine_->free_samples(false));
     }
     return finish(res);
 }
@@ -1743,6 +1764,7 @@ int Job::step(uint32_t rounds, silvan_status_t *st, FILE *sink) {
         own_engine_->reset_timers();
         launches = 0;
         RK(begin(sink, own_engine_->stream()));
+        set_lookahead(own_engine_->free_samples(true), own_engine_->free_samples(false));
     }
     std::vector<Job *> jobs{this};
     std::vector<JobRequest> reqs(1);
@@ -1758,7 +1780,7 @@ int Job::step(uint32_t rounds, silvan_status_t *st, FILE *sink) {
             error_ = rc;
             return rc;
         }
-        lookahead_ = own_engine_->free_samples();
+        set_lookahead(own_engine_->free_samples(true), own_engine_->free_samples(false));
     }
     if (st) {
         JobScalars sc{};
@@ -1816,8 +1838,9 @@ int run_batched(const std::vector<Job *> &jobs, uint64_t mem_budget, silvan_resu
         std::vector<uint64_t> nrec;
         RK(eng.round(act, reqs, nrec));
         for (size_t i = 0; i < act.size(); i++) RK(act[i]->on_drawn(reqs[i], nrec[i]));
-        const uint32_t la = eng.free_samples() / std::max<size_t>(1, act.size());
-        for (Job *j : act) j->set_lookahead(la);
+        const size_t na = std::max<size_t>(1, act.size());
+        for (Job *j : act)
+            j->set_lookahead(eng.free_samples(true) / na, eng.free_samples(false) / na);
     }
     for (size_t i = 0; i < jobs.size(); i++) RK(jobs[i]->finish(&results[i]));
     return SILVAN_OK;
@@ -1891,6 +1914,7 @@ int Job::replay(uint32_t first, uint32_t count, double alpha, std::vector<int32_
         reqs[0].first_global = first + done;
         reqs[0].count = c;
         reqs[0].pass = 1;
+        reqs[0].alpha = alpha;
         RK(own_engine_->round(jobs, reqs, nrec));
         CK(cudaMemcpy(pl.data() + done, rb_.pl, sizeof(int32_t) * c, cudaMemcpyDeviceToHost));
         CK(cudaMemcpy(np.data() + done, rb_.np, sizeof(int32_t) * c, cudaMemcpyDeviceToHost));

@@ -88,6 +88,7 @@ struct JobRequest {
     uint32_t count = 0;
     int pass = 1;
     bool track_cross = false;
+    double alpha = 0;           // multi-path rate the range is drawn with
 };
 
 class Job;
@@ -114,10 +115,10 @@ class Engine {
     // receives the number of path-map records of each job.
     int round(const std::vector<Job *> &jobs, const std::vector<JobRequest> &reqs,
               std::vector<uint64_t> &records);
-    // samples that one more launch could draw for free: a launch lasts about
-    // as long as its slowest sample, during which the other slots keep
+    // samples that one more launch could draw for free: a launch lasts at
+    // least as long as its slowest sample, during which the other slots keep
     // drawing (0 until a launch has been measured)
-    uint32_t free_samples() const;
+    uint32_t free_samples(bool tail_only) const;
     uint64_t launches() const { return launches_; }
     float sample_ms() const { return sample_ms_; }
     void reset_timers() {
@@ -171,6 +172,7 @@ class Engine {
     uint64_t launches_ = 0;
     double clock_khz_ = 0;
     double last_cta_ms_ = 0;     // CTA ms per sample of the last launch
+    double last_tail_ms_ = 0;    // its slowest sample
     double last_launch_ms_ = 0;
     uint32_t last_grid_ = 0;
 };
@@ -194,7 +196,12 @@ class Job {
     // after the engine drew the requested range: commits it schedule point by
     // schedule point and evaluates each point
     int on_drawn(const JobRequest &r, uint64_t n_records);
-    void set_lookahead(uint32_t samples) { lookahead_ = samples; }
+    // speculative draw sizes: within the slowest sample's time (first pass)
+    // and within the last launch's time (second pass, capped by omega)
+    void set_lookahead(uint32_t tail, uint32_t launch) {
+        lookahead_tail_ = tail;
+        lookahead_ = launch;
+    }
     int finish(silvan_result_t *res);
     int error() const { return error_; }
     uint32_t nodes() const { return n_; }
@@ -271,7 +278,9 @@ class Job {
     uint32_t k_ = 0, union_sample_ = 0, tau_ = 0;
     uint64_t base_global_ = 0;   // global index of the pass's first sample
     uint32_t lookahead_ = 0;     // pass 2: samples drawn ahead of the next point
+    uint32_t lookahead_tail_ = 0;  // pass 1 (absolute mode): samples drawn beyond it
     float commit_ms_ = 0;
+    uint64_t drawn_ = 0;         // samples drawn over both passes
     cudaEvent_t ev_commit_[2] = {nullptr, nullptr};
     uint64_t pass_samples_ = 0;  // samples committed in the current pass
     uint64_t target_ = 0;        // sample count of the next schedule event
