@@ -818,6 +818,7 @@ Job::~Job() {
     hfree(h_state_);
     hfree(h_red_);
     hfree(h_sc_);
+    hfree(h_sp_);
     for (auto &e : ev_run_)
         if (e) cudaEventDestroy(e);
     for (auto &e : ev_commit_)
@@ -906,6 +907,7 @@ int Job::init() {
     RK(hmalloc(&h_state_, kArgRing));
     RK(hmalloc(&h_red_, 1));
     RK(hmalloc(&h_sc_, 1));
+    RK(hmalloc(&h_sp_, (size_t)g_->diameter + 1));
     CK(cudaMemset(jc_.approx, 0, sizeof(double) * n));
     CK(cudaMemset(jc_.wimpy, 0, sizeof(double) * n));
     CK(cudaMemset(jc_.mcrade, 0, sizeof(long long) * (uint64_t)n * kTrials));
@@ -1242,13 +1244,16 @@ int Job::stop_check(bool &stop) {
     const long long init = -(long long)pass_samples_;
     CK(stop_reduce(jc_, nparts_, init, d_red_, stream_));
     launches += 2;
+    // the reduction, the shortest-path lengths and the scalars in one round trip
     CK(cudaMemcpyAsync(h_red_, d_red_, sizeof(StopReduction), cudaMemcpyDeviceToHost, stream_));
+    if (absolute_)
+        CK(cudaMemcpyAsync(h_sp_, jc_.sp_lengths, sizeof(uint64_t) * ((size_t)g_->diameter + 1),
+                           cudaMemcpyDeviceToHost, stream_));
     JobScalars sc;
     RK(sync_scalars(sc));
     const StopReduction &R = *h_red_;
     if (absolute_) {
-        std::vector<uint64_t> sp;
-        RK(read_sp_lengths(sp));
+        const std::vector<uint64_t> sp(h_sp_, h_sp_ + g_->diameter + 1);
         const double adu = upper_bound_avg_diameter(sp, (int)g_->diameter, dpb, pass_samples_).ub;
         const double t1 = R.approx_max / ms;
         const double t1u = upper_bound_top1(t1, dpb, pass_samples_);

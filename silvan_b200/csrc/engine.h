@@ -262,6 +262,7 @@ class Job {
     StopReduction *d_red_ = nullptr;
     StopReduction *h_red_ = nullptr;  // pinned
     JobScalars *h_sc_ = nullptr;      // pinned
+    uint64_t *h_sp_ = nullptr;        // pinned, diameter + 1 shortest-path lengths
     uint32_t *d_unc_ = nullptr, *d_nunc_ = nullptr;
     int32_t *d_lut_ = nullptr;
     uint32_t *d_hist_ = nullptr;
