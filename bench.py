@@ -227,6 +227,21 @@ def cpu_reference(lib, csr, cfg, threads):
     return r, what
 
 
+def combine_replicas(pg, samples, t_dev, e2e_samples, e2e_t, device="cpu"):
+    """Replicas on N ranks: total samples over all ranks, time of the slowest
+    rank (the same for the end-to-end leg).  `pg` is torch.distributed (or
+    None for one rank); every rank takes the same two collectives."""
+    import torch
+    if pg is None:
+        return samples, t_dev, e2e_samples, e2e_t
+    vals = torch.tensor([samples, t_dev, e2e_samples, e2e_t], dtype=torch.float64, device=device)
+    tot = vals.clone()
+    mx = vals.clone()
+    pg.all_reduce(tot)
+    pg.all_reduce(mx, op=pg.ReduceOp.MAX)
+    return tot[0].item(), mx[1].item(), tot[2].item(), mx[3].item()
+
+
 def dist_env():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -693,17 +708,8 @@ def main():
         e2e_samples += r["first_pass_samples"] + r["num_samples"]
         del job, g2
 
-    # aggregate over ranks: total work / slowest rank
-    vals = torch.tensor([samples, t_dev, e2e_samples, e2e_t], dtype=torch.float64, device="cuda")
-    if pg:
-        tot = vals.clone()
-        mx = vals.clone()
-        pg.all_reduce(tot)
-        pg.all_reduce(mx, op=pg.ReduceOp.MAX)
-        samples_all, t_max, e2e_s_all, e2e_t_max = tot[0].item(), mx[1].item(), tot[2].item(), \
-            mx[3].item()
-    else:
-        samples_all, t_max, e2e_s_all, e2e_t_max = samples, t_dev, e2e_samples, e2e_t
+    samples_all, t_max, e2e_s_all, e2e_t_max = combine_replicas(
+        pg, samples, t_dev, e2e_samples, e2e_t, device="cuda")
     if rank == 0:
         peak, peak_kind = peaks()
         # roofline of the sampler kernel: algorithmic bytes per sample are
