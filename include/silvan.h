@@ -128,6 +128,7 @@ typedef struct {
     uint64_t kernel_launches;    /* kernels launched by the run             */
     uint32_t sampler_launches;   /* persistent sampler launches (own engine) */
     uint32_t sampler_block;      /* CTA size that drew most samples          */
+    uint64_t samples_drawn;      /* samples drawn, speculative ones included */
 } silvan_result_t;
 
 /* ---- graphs (reference: Graph, silvan/src/Graph.cpp) ------------------- */
@@ -283,6 +284,14 @@ int silvan_server_estimates(silvan_server_t s, uint64_t id, double *out, uint32_
                             uint32_t *topk_count);
 int silvan_server_stats(silvan_server_t s, silvan_server_stats_t *st);
 int silvan_server_destroy(silvan_server_t s);
+
+/* ---- exact betweenness (validation) --------------------------------------- */
+
+/* Exact betweenness of every node (Brandes, on the device), normalised by
+ * n (n - 1) over ordered pairs: the quantity the estimator approximates, for
+ * checking the (eps, delta) guarantee.  No counterpart in the reference,
+ * which has no exact algorithm.  out has n entries. */
+int silvan_exact_betweenness(silvan_graph_t g, double *out, uint32_t n);
 
 /* ---- per-sample replay (parity hook) -------------------------------------- */
 

@@ -37,7 +37,7 @@ EXPORTS = [
     "silvan_graph_from_pairs", "silvan_last_error", "silvan_version", "silvan_job_result",
     "silvan_jobs_run_batched", "silvan_server_create", "silvan_server_submit",
     "silvan_server_poll", "silvan_server_wait", "silvan_server_estimates", "silvan_server_stats",
-    "silvan_server_destroy", "silvan_replay_samples_noalloc",
+    "silvan_server_destroy", "silvan_replay_samples_noalloc", "silvan_exact_betweenness",
 ]
 
 REQ_QUEUED, REQ_RUNNING, REQ_DONE = 1, 2, 3
@@ -322,6 +322,12 @@ class Graph:
         _check(load().silvan_graph_csr(self.h, _p(oo), _p(oa), _p(io), _p(ia), _p(cc)))
         return CSR(n, bool(i.directed), oo, oa[:int(oo[-1])], io, ia[:int(io[-1])], cc,
                    i.n_components, i.diameter)
+
+    def exact_betweenness(self):
+        """Exact normalised betweenness of every node (Brandes on the device)."""
+        out = np.zeros(self.n, np.float64)
+        _check(load().silvan_exact_betweenness(self.h, _p(out), self.n))
+        return out
 
     def replay(self, seed, first, count, alpha, np_cap=0):
         """Per-sample output of the device sampler for samples

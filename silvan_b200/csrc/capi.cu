@@ -7,6 +7,7 @@
 
 #include "engine.h"
 #include "ingest.h"
+#include "brandes.h"
 #include "gen.h"
 #include "server.h"
 #include "silvan.h"
@@ -561,6 +562,18 @@ int silvan_replay_samples(silvan_graph_t g, uint64_t seed, uint32_t first, uint3
         if (ent_cnt) ent_cnt[i] = (int32_t)recs[i].count;
     }
     return SILVAN_OK;
+}
+
+int silvan_exact_betweenness(silvan_graph_t g, double *out, uint32_t n) {
+    if (!g || !out) {
+        set_error("null argument");
+        return SILVAN_E_BADARG;
+    }
+    if (n != g->g.n) {
+        set_error("output size does not match the graph");
+        return SILVAN_E_BADARG;
+    }
+    return exact_betweenness(g->g, out);
 }
 
 int silvan_replay_samples_noalloc(silvan_graph_t g, uint64_t seed, uint32_t first,
