@@ -1,12 +1,13 @@
 // Estimation server: continuous batching of progressive-sampling jobs.
 //
 // Requests (a host graph plus the binary's flags) are queued by any thread.
-// One server thread owns the device: it admits queued requests in arrival
-// order while their device memory (CSR + counters + round buffers) fits the
-// budget, keeps every admitted job's graph and state on the device, and runs
-// rounds: each round is one persistent sampler launch serving the next
-// schedule interval of every active job, followed by each job's ordered
-// commit and schedule evaluation (engine.cu).  A job that reaches its
+// An uploader thread admits queued requests in arrival order while their
+// device memory (CSR + counters + round buffers) fits the budget and puts
+// each admitted job's graph and state on the device; the server thread keeps
+// them there and runs rounds: each round is one persistent sampler launch
+// serving the next schedule interval of every active job, followed by each
+// job's ordered commit and schedule evaluation (engine.cu).  Uploads overlap
+// the rounds of the requests already running.  A job that reaches its
 // stopping decision releases its memory, its estimates are copied to the host
 // and the next queued request can be admitted -- requests arriving while
 // others run join at the next round.  Each job follows exactly its stand-alone
@@ -55,11 +56,14 @@ struct Server {
     std::mutex mu;
     std::condition_variable cv;
     std::deque<ServerRequest *> pending;
+    std::deque<ServerRequest *> ready;      // uploaded, waiting for the server thread
     std::vector<ServerRequest *> active;
+    uint64_t in_upload = 0;                 // admitted, not yet ready
     std::map<uint64_t, std::unique_ptr<ServerRequest>> all;
     uint64_t next_id = 1;
     std::atomic<bool> stop{false};
-    std::thread th;
+    std::thread th, up_th;
+    int device = 0;
     int fatal = 0;
     uint64_t rounds = 0, max_active = 0, samples = 0;
     int init_rc = SILVAN_OK;
@@ -94,35 +98,19 @@ struct Server {
         std::vector<Job *> jobs;
         std::vector<JobRequest> reqs;
         while (!stop.load()) {
-            // admission by device-memory budget, in arrival order
-            std::vector<ServerRequest *> admit;
+            // requests whose graph and state the uploader has put on the device
+            std::vector<ServerRequest *> start;
             {
                 std::unique_lock<std::mutex> lk(mu);
-                if (active.empty() && pending.empty())
+                if (active.empty() && ready.empty())
                     cv.wait_for(lk, std::chrono::milliseconds(20));
-                while (!pending.empty()) {
-                    ServerRequest *r = pending.front();
-                    if (used + r->bytes > budget && !(active.empty() && admit.empty())) break;
-                    pending.pop_front();
-                    used += r->bytes;
-                    r->state = SILVAN_REQ_RUNNING;
-                    r->t_admit = now_seconds();
-                    admit.push_back(r);
+                while (!ready.empty()) {
+                    start.push_back(ready.front());
+                    ready.pop_front();
                 }
             }
-            const double t_adm = now_seconds();
-            for (ServerRequest *r : admit) {
-                r->graph.reset(new DeviceGraph());
-                r->graph->host = std::move(r->host);
-                r->graph->cc = std::move(r->cc);
-                r->graph->ncomp = r->ncomp;
-                r->graph->diameter = r->diameter;
-                int rc = r->graph->upload();
-                if (rc == SILVAN_OK) {
-                    r->job.reset(new Job(r->graph.get(), r->params));
-                    rc = r->job->init();
-                }
-                if (rc == SILVAN_OK) rc = r->job->begin(nullptr, eng.stream());
+            for (ServerRequest *r : start) {
+                int rc = r->job->begin(nullptr, eng.stream());
                 if (rc != SILVAN_OK) {
                     finish(r, rc);
                     continue;
@@ -130,7 +118,6 @@ struct Server {
                 std::lock_guard<std::mutex> lk(mu);
                 active.push_back(r);
             }
-            if (!admit.empty()) account(0, t_adm);
             if (active.empty()) continue;
             max_active = std::max<uint64_t>(max_active, active.size());
             jobs.clear();
@@ -172,6 +159,60 @@ struct Server {
                 if (e != SILVAN_OK) finish(r, e);
                 else if (r->job->done()) finish(r, SILVAN_OK);
             }
+        }
+    }
+
+    // Admission by device-memory budget, in arrival order, and the upload of
+    // each admitted request's graph and job state, on a thread of its own so
+    // that the rounds of the active requests go on meanwhile (the copies run
+    // on the legacy stream, the rounds on the engine's non-blocking stream).
+    void uploader() {
+        cudaSetDevice(device);
+        while (!stop.load()) {
+            ServerRequest *r = nullptr;
+            {
+                std::unique_lock<std::mutex> lk(mu);
+                cv.wait_for(lk, std::chrono::milliseconds(20), [this]() {
+                    return stop.load() || (!pending.empty() &&
+                                           (used + pending.front()->bytes <= budget ||
+                                            (active.empty() && ready.empty() && !in_upload)));
+                });
+                if (stop.load() || pending.empty()) continue;
+                r = pending.front();
+                if (used + r->bytes > budget && !(active.empty() && ready.empty() && !in_upload))
+                    continue;
+                pending.pop_front();
+                used += r->bytes;
+                in_upload++;
+                r->state = SILVAN_REQ_RUNNING;
+                r->t_admit = now_seconds();
+            }
+            const double t_adm = now_seconds();
+            r->graph.reset(new DeviceGraph());
+            r->graph->host = std::move(r->host);
+            r->graph->cc = std::move(r->cc);
+            r->graph->ncomp = r->ncomp;
+            r->graph->diameter = r->diameter;
+            int rc = r->graph->upload();
+            if (rc == SILVAN_OK) {
+                r->job.reset(new Job(r->graph.get(), r->params));
+                rc = r->job->init();
+            }
+            // the upload and the set-up ran on the legacy stream: done before the
+            // request's first round on the engine's stream
+            if (rc == SILVAN_OK)
+                rc = cuda_status(cudaStreamSynchronize(cudaStreamLegacy), "request upload");
+            account(0, t_adm);
+            if (rc != SILVAN_OK) {
+                finish(r, rc);
+                std::lock_guard<std::mutex> lk(mu);
+                in_upload--;
+                continue;
+            }
+            std::lock_guard<std::mutex> lk(mu);
+            in_upload--;
+            ready.push_back(r);
+            cv.notify_all();
         }
     }
 
@@ -224,6 +265,7 @@ int server_create(uint64_t n_max, uint64_t budget, uint32_t slots, Server **out)
         budget = fr / 3;
     }
     s->budget = budget;
+    s->device = dev;
     s->th = std::thread([s, dev]() { s->loop(dev); });
     std::unique_lock<std::mutex> lk(s->init_mu);
     s->init_cv.wait(lk, [s]() { return s->init_done; });
@@ -235,6 +277,7 @@ int server_create(uint64_t n_max, uint64_t budget, uint32_t slots, Server **out)
         delete s;
         return rc;
     }
+    s->up_th = std::thread([s]() { s->uploader(); });
     *out = s;
     return SILVAN_OK;
 }
@@ -352,6 +395,7 @@ int server_stats(Server *s, silvan_server_stats_t *st) {
 void server_destroy(Server *s) {
     s->stop = true;
     s->cv.notify_all();
+    if (s->up_th.joinable()) s->up_th.join();
     if (s->th.joinable()) s->th.join();
     for (auto &kv : s->all) {
         kv.second->job.reset();
