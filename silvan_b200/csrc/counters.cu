@@ -272,7 +272,11 @@ __global__ void __launch_bounds__(kApplyThreads) apply_small_kernel(const ApplyS
     for (uint32_t t = gw; t < T; t += nw) {
         const uint32_t b0 = rb.bucket_off[t];
         const uint32_t b = rb.bucket_off[t + 1] - b0;
-        if (b > 32) continue;
+        if (b > 32) {
+            // for apply_large, which then visits only these
+            if (lane == 0) rb.large[atomicAdd(rb.n_large, 1u)] = t;
+            continue;
+        }
         const uint32_t node = rb.touched[t];
         unsigned long long key = (uint32_t)lane < b ? rb.entries[b0 + lane] : ~0ull;
         warp_bitonic_sort(key);
@@ -291,11 +295,11 @@ __global__ void __launch_bounds__(1024) apply_large_kernel(const ApplyState *st)
     const RoundBuffers rb = st->rb;
     const JobCounters jc = st->jc;
     const ApplyArgs a = st->a;
-    const uint32_t T = *rb.n_touched;
-    for (uint32_t t = blockIdx.x; t < T; t += gridDim.x) {
+    const uint32_t NL = *rb.n_large;
+    for (uint32_t li = blockIdx.x; li < NL; li += gridDim.x) {
+        const uint32_t t = rb.large[li];
         const uint32_t b0 = rb.bucket_off[t];
         const uint32_t b = rb.bucket_off[t + 1] - b0;
-        if (b <= 32) continue;
         if (b > kLargeBucket) {
             if (threadIdx.x == 0) atomicCAS(&jc.sc->error, 0, SILVAN_E_CAPACITY);
             continue;
@@ -499,7 +503,7 @@ cudaError_t apply_init() {
 }
 
 cudaError_t apply_round(const ApplyState *st, uint32_t *n_touched, cudaStream_t stream) {
-    cudaMemsetAsync(n_touched, 0, sizeof(uint32_t), stream);
+    cudaMemsetAsync(n_touched, 0, 2 * sizeof(uint32_t), stream);  // n_touched, n_large
     signs_kernel<<<64, 256, 0, stream>>>(st);
     bucket_count_kernel<<<592, 256, 0, stream>>>(st);
     scan_reduce_kernel<<<kScanBlocks, kScanThreads, 0, stream>>>(st);

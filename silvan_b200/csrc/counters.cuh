@@ -48,6 +48,8 @@ struct RoundBuffers {
     uint32_t *touched;       // distinct nodes of the round
     uint32_t *n_touched;
     uint32_t *bucket_off;    // n_touched + 1
+    uint32_t *large;         // buckets of more than 32 entries (listed by apply_small)
+    uint32_t *n_large;       // = n_touched + 1 (both zeroed together)
     unsigned long long *entries;  // sample << 32 | count, grouped by node
     uint32_t *block_sums;    // scan scratch
     uint32_t *work_counter;  // sampler work counter

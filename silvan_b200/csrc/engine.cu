@@ -794,6 +794,7 @@ Job::~Job() {
     dfree(r.recs);
     dfree(r.node_cnt);
     dfree(r.touched);
+    dfree(r.large);
     dfree(r.n_touched);
     dfree(r.bucket_off);
     dfree(r.entries);
@@ -836,7 +837,8 @@ int Job::alloc_round(uint32_t max_samples, uint64_t rec_cap) {
     RK(dmalloc(&r.ball, max_samples));
     RK(dmalloc(&r.pred, max_samples));
     RK(dmalloc(&r.node_cnt, n_));
-    RK(dmalloc(&r.n_touched, 1));
+    RK(dmalloc(&r.n_touched, 2));
+    r.n_large = r.n_touched + 1;
     RK(dmalloc(&r.block_sums, 1024));
     r.rec_cursor = nullptr;
     r.work_counter = nullptr;
@@ -849,12 +851,14 @@ int Job::grow_records(uint64_t cap) {
     if (stream_) cudaStreamSynchronize(stream_);
     dfree(r.recs);
     dfree(r.touched);
+    dfree(r.large);
     dfree(r.bucket_off);
     dfree(r.entries);
     r.rec_cap = cap;
     const uint64_t tcap = std::min<uint64_t>(cap, n_) + 1;
     RK(dmalloc(&r.recs, cap));
     RK(dmalloc(&r.touched, tcap));
+    RK(dmalloc(&r.large, tcap));
     RK(dmalloc(&r.bucket_off, tcap + 1));
     RK(dmalloc(&r.entries, cap));
     return SILVAN_OK;
