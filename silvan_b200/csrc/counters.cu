@@ -517,6 +517,17 @@ cudaError_t apply_round(const ApplyState *st, uint32_t *n_touched, cudaStream_t 
     return cudaGetLastError();
 }
 
+__global__ void divide_kernel(const double *approx, double m, double *out, uint32_t n) {
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x)
+        out[v] = __ddiv_rn(approx[v], m);
+}
+
+cudaError_t divide_estimates(const double *approx, double num_samples, double *out, uint32_t n,
+                             cudaStream_t stream) {
+    divide_kernel<<<592, 256, 0, stream>>>(approx, num_samples, out, n);
+    return cudaGetLastError();
+}
+
 cudaError_t stop_reduce(const JobCounters &jc, int nparts, long long init,
                         StopReduction *out_dev, cudaStream_t stream) {
     stop_init_kernel<<<1, 256, 0, stream>>>(out_dev, nparts, init);

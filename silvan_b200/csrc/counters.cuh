@@ -112,6 +112,10 @@ struct StopReduction {
     double approx_max;
     double wimpy_all_max;
 };
+// out[v] = approx[v] / num_samples (the estimates the reference prints).
+cudaError_t divide_estimates(const double *approx, double num_samples, double *out, uint32_t n,
+                             cudaStream_t stream);
+
 cudaError_t stop_reduce(const JobCounters &jc, int nparts, long long init,
                         StopReduction *out_dev, cudaStream_t stream);
 

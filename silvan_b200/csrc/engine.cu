@@ -268,45 +268,62 @@ int DeviceGraph::upload_raw(uint32_t nn, bool dir, const uint64_t *out_off,
         return SILVAN_E_BADARG;
     }
     CK(cudaGetDevice(&device));
-    uint64_t *tmp = nullptr;
+    // the two directions go up on two streams, so that their copies can use
+    // two copy engines and each one's checks overlap the other's copies
+    cudaStream_t st[2] = {nullptr, nullptr};
+    uint64_t *tmp[2] = {nullptr, nullptr};
     uint32_t *bad = nullptr;
-    RK(dmalloc(&tmp, (size_t)nn + 1));
+    struct Cleanup {
+        cudaStream_t *st;
+        uint64_t **tmp;
+        uint32_t **bad;
+        ~Cleanup() {
+            for (int i = 0; i < 2; i++)
+                if (st[i]) {
+                    cudaStreamSynchronize(st[i]);
+                    cudaStreamDestroy(st[i]);
+                }
+            dfree(tmp[0]);
+            dfree(tmp[1]);
+            dfree(*bad);
+        }
+    } cleanup{st, tmp, &bad};
+    for (int i = 0; i < 2; i++) CK(cudaStreamCreateWithFlags(&st[i], cudaStreamNonBlocking));
+    RK(dmalloc(&tmp[0], (size_t)nn + 1));
+    RK(dmalloc(&tmp[1], (size_t)nn + 1));
     RK(dmalloc(&bad, 1));
-    auto put = [&](uint32_t **doff, uint32_t **dadj, const uint64_t *off, const uint32_t *adj,
-                   uint64_t cnt) -> int {
+    CK(cudaMemsetAsync(bad, 0, sizeof(uint32_t), st[0]));
+    CK(cudaStreamSynchronize(st[0]));
+    auto put = [&](int i, uint32_t **doff, uint32_t **dadj, const uint64_t *off,
+                   const uint32_t *adj, uint64_t cnt) -> int {
         RK(dmalloc(doff, (size_t)nn + 1));
         RK(dmalloc(dadj, cnt));
-        CK(cudaMemcpy(tmp, off, sizeof(uint64_t) * (nn + 1), cudaMemcpyHostToDevice));
-        CK(narrow_offsets(tmp, *doff, nn + 1, 0));
-        if (cnt) CK(cudaMemcpy(*dadj, adj, sizeof(uint32_t) * cnt, cudaMemcpyHostToDevice));
-        CK(validate_rows(*doff, *dadj, nn, bad, 0));
+        CK(cudaMemcpyAsync(tmp[i], off, sizeof(uint64_t) * (nn + 1), cudaMemcpyHostToDevice,
+                           st[i]));
+        CK(narrow_offsets(tmp[i], *doff, nn + 1, st[i]));
+        if (cnt)
+            CK(cudaMemcpyAsync(*dadj, adj, sizeof(uint32_t) * cnt, cudaMemcpyHostToDevice, st[i]));
+        CK(validate_rows(*doff, *dadj, nn, bad, st[i]));
         return SILVAN_OK;
     };
-    CK(cudaMemset(bad, 0, sizeof(uint32_t)));
-    int rc = put(&d_out_off, &d_out_adj, out_off, out_adj, m);
-    if (rc == SILVAN_OK) {
-        if (dir) {
-            rc = put(&d_in_off, &d_in_adj, in_off, in_adj, m_in);
-        } else {
-            d_in_off = d_out_off;
-            d_in_adj = d_out_adj;
-        }
+    RK(dmalloc(&d_cc, nn));
+    RK(put(0, &d_out_off, &d_out_adj, out_off, out_adj, m));
+    if (dir) {
+        RK(put(1, &d_in_off, &d_in_adj, in_off, in_adj, m_in));
+    } else {
+        d_in_off = d_out_off;
+        d_in_adj = d_out_adj;
     }
-    if (rc == SILVAN_OK) rc = dmalloc(&d_cc, nn);
-    if (rc == SILVAN_OK)
-        rc = cuda_status(cudaMemcpy(d_cc, cc_in, sizeof(uint32_t) * nn, cudaMemcpyHostToDevice),
-                         "cc upload");
+    CK(cudaMemcpyAsync(d_cc, cc_in, sizeof(uint32_t) * nn, cudaMemcpyHostToDevice, st[1]));
+    CK(cudaStreamSynchronize(st[0]));
+    CK(cudaStreamSynchronize(st[1]));
     uint32_t hbad = 0;
-    if (rc == SILVAN_OK)
-        rc = cuda_status(cudaMemcpy(&hbad, bad, sizeof(uint32_t), cudaMemcpyDeviceToHost),
-                         "validation");
-    dfree(tmp);
-    dfree(bad);
-    if (rc == SILVAN_OK && hbad) {
+    CK(cudaMemcpy(&hbad, bad, sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    if (hbad) {
         set_error("CSR rows must hold ascending unique ids < n");
-        rc = SILVAN_E_BADARG;
+        return SILVAN_E_BADARG;
     }
-    return rc;
+    return SILVAN_OK;
 }
 
 uint64_t DeviceGraph::device_bytes() const {
@@ -1863,9 +1880,14 @@ int Job::read_estimates(double *out, uint32_t n) {
         set_error("estimate buffer size does not match the graph");
         return SILVAN_E_BADARG;
     }
-    CK(cudaMemcpy(out, jc_.approx, sizeof(double) * n, cudaMemcpyDeviceToHost));
-    const double ms = (double)pass_samples_;
-    for (uint32_t i = 0; i < n; i++) out[i] = out[i] / ms;
+    // approx / num_samples on the device (the same IEEE division), then one copy
+    double *est = nullptr;
+    RK(dmalloc(&est, n));
+    CK(divide_estimates(jc_.approx, (double)pass_samples_, est, n, stream_));
+    cudaError_t e = cudaMemcpyAsync(out, est, sizeof(double) * n, cudaMemcpyDeviceToHost, stream_);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
+    dfree(est);
+    CK(e);
     return SILVAN_OK;
 }
 
