@@ -294,7 +294,9 @@ def run_reference_arm(args, cfg):
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1000 * t / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u32/u64/f64", "data": "synthetic",
-        "config": {"workload": cfg["workload"], "eps": cfg.get("eps"), "delta": cfg["delta"]},
+        "config": dict({"workload": cfg["workload"], "eps": cfg.get("eps"), "delta": cfg["delta"],
+                        "form": "reference OpenMP build", "parallelism": "host threads"},
+                       **({} if cfg["kind"] == "multi" else job_kwargs(cfg))),
         "time_to_guarantee_ms": 1000 * t / args.steps,
         "cpu_baseline": {"value": val, "unit": "paths/s", "cores": threads, "kind": "reference",
                          "sample": f"{args.steps} x ({what})"},
