@@ -25,7 +25,7 @@ BIN = os.path.join(PKG, "bin", "silvan")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 SOURCES = ["graph_host.cpp", "gen.cpp", "graph_dev.cu", "sampler.cu", "counters.cu", "engine.cu",
-           "server.cu", "noalloc.cu", "ingest.cu", "brandes.cu", "capi.cu"]
+           "server.cu", "noalloc.cu", "ingest.cu", "components.cu", "brandes.cu", "capi.cu"]
 
 
 def _nvcc():

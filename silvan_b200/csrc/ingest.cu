@@ -18,9 +18,10 @@
 // gives the CSR.  The scans, the select, the sort and the unique are CUB's
 // device primitives; the parsing and CSR kernels are this file's.
 //
-// The CSR stays on the device; a host copy is read back for the strongly
-// connected components and the diameter bound, which run on the host
-// (graph_host.cpp), and for silvan_graph_csr.
+// The CSR stays on the device.  For an undirected graph the components and
+// the diameter bound are computed there too (components.cu); for a directed
+// graph a host copy is read back for the reference's Tarjan numbering and the
+// bound (graph_host.cpp).
 #include <cub/cub.cuh>
 #include <thrust/iterator/counting_iterator.h>
 #include <thrust/iterator/transform_iterator.h>
@@ -31,6 +32,7 @@
 
 #include "engine.h"
 #include "ingest.h"
+#include "components.h"
 
 namespace silvan {
 
@@ -183,7 +185,8 @@ struct Scratch {
 // Sorted unique keys -> CSR (u32 offsets) on the device and the host copy.
 int keys_to_device_csr(Scratch &S, uint64_t *keys, uint64_t count, uint32_t n, int end_bit,
                        cudaStream_t st, uint32_t **d_off, uint32_t **d_adj, uint64_t *m_out,
-                       std::vector<uint64_t> &h_off, std::vector<uint32_t> &h_adj) {
+                       std::vector<uint64_t> &h_off, std::vector<uint32_t> &h_adj,
+                       bool host_copy) {
     uint64_t *sorted = nullptr, *uniq = nullptr, *d_m = nullptr;
     RKI(S.get(&sorted, count));
     RKI(S.get(&uniq, count));
@@ -206,15 +209,19 @@ int keys_to_device_csr(Scratch &S, uint64_t *keys, uint64_t count, uint32_t n, i
     RKI(dalloc(d_adj, m));
     csr_offsets_kernel<<<1184, 256, 0, st>>>(uniq, m, n, *d_off, *d_adj);
     CKI(cudaGetLastError());
-    std::vector<uint32_t> off32((size_t)n + 1);
-    h_adj.resize(m);
-    CKI(cudaMemcpyAsync(off32.data(), *d_off, sizeof(uint32_t) * ((size_t)n + 1),
-                        cudaMemcpyDeviceToHost, st));
-    if (m)
-        CKI(cudaMemcpyAsync(h_adj.data(), *d_adj, sizeof(uint32_t) * m, cudaMemcpyDeviceToHost,
-                            st));
-    CKI(cudaStreamSynchronize(st));
-    h_off.assign(off32.begin(), off32.end());
+    if (host_copy) {
+        std::vector<uint32_t> off32((size_t)n + 1);
+        h_adj.resize(m);
+        CKI(cudaMemcpyAsync(off32.data(), *d_off, sizeof(uint32_t) * ((size_t)n + 1),
+                            cudaMemcpyDeviceToHost, st));
+        if (m)
+            CKI(cudaMemcpyAsync(h_adj.data(), *d_adj, sizeof(uint32_t) * m,
+                                cudaMemcpyDeviceToHost, st));
+        CKI(cudaStreamSynchronize(st));
+        h_off.assign(off32.begin(), off32.end());
+    } else {
+        CKI(cudaStreamSynchronize(st));
+    }
     *m_out = m;
     return SILVAN_OK;
 }
@@ -361,12 +368,15 @@ int device_ingest(const char *path, bool directed, DeviceGraph &G, std::string &
     }
     int end_bit = 32;
     while (end_bit < 64 && ((uint64_t)(n - 1) >> (end_bit - 32)) != 0) end_bit++;
+    // undirected graphs: components and diameter bound on the device too, no
+    // host copy; directed graphs: the reference's Tarjan numbering on the host
+    const bool host_copy = directed;
     uint64_t m = 0, m_in = 0;
     RKI(keys_to_device_csr(S, out_keys, n_out, n, end_bit, st, &G.d_out_off, &G.d_out_adj, &m,
-                           G.host.out_off, G.host.out_adj));
+                           G.host.out_off, G.host.out_adj, host_copy));
     if (directed) {
         RKI(keys_to_device_csr(S, in_keys, edges, n, end_bit, st, &G.d_in_off, &G.d_in_adj, &m_in,
-                               G.host.in_off, G.host.in_adj));
+                               G.host.in_off, G.host.in_adj, host_copy));
     } else {
         G.d_in_off = G.d_out_off;
         G.d_in_adj = G.d_out_adj;
@@ -376,9 +386,16 @@ int device_ingest(const char *path, bool directed, DeviceGraph &G, std::string &
     }
     G.m = m;
     G.m_in = m_in;
-    G.has_host = true;
     CKI(cudaGetDevice(&G.device));
-    return G.finish_from_host_copy();
+    if (directed) {
+        G.has_host = true;
+        return G.finish_from_host_copy();
+    }
+    G.has_host = false;
+    const double t0 = now_seconds();
+    RKI(device_undirected_components(G, st));
+    G.diameter_seconds = now_seconds() - t0;
+    return SILVAN_OK;
 }
 
 }  // namespace silvan

@@ -95,3 +95,20 @@ def test_estimation_on_device_loaded_graph(sb, tmp_path):
     ra, rb = a.run(), b.run()
     assert ra["num_samples"] == rb["num_samples"]
     np.testing.assert_array_equal(a.get_centrality(), b.get_centrality())
+
+
+@pytest.mark.parametrize("make", [
+    lambda sb: sb.grid(64, 0.45, 0.0, 5),          # a lattice broken into many pieces
+    lambda sb: sb.rmat(14, 4, 9, False),           # R-MAT with isolated ids
+    lambda sb: sb.erdos_renyi(3000, 1.2, 4),       # near the percolation threshold
+])
+def test_undirected_components_on_the_device(sb, tmp_path, make):
+    """Undirected graphs get their component numbers and diameter bound on
+    the device (Tarjan's numbering is the order of the components' smallest
+    ids); they must equal the host's restatement of the reference."""
+    path = str(tmp_path / "u.txt")
+    sb.write_edge_list(path, make(sb))
+    dev = sb.Graph.load(path, False).csr()
+    host = sb.HostGraph.load(path, False).csr()
+    assert host.n_components > 10
+    assert_same_graph(dev, host)
