@@ -17,6 +17,15 @@
 
 namespace silvan {
 
+// Held while a stream is being captured into a CUDA graph and around every
+// call that synchronises the whole device or maps and unmaps memory: such a
+// call from another thread would invalidate a capture in progress (the
+// server's uploader thread allocates while its round thread captures).
+std::mutex &capture_mutex() {
+    static std::mutex *m = new std::mutex();
+    return *m;
+}
+
 namespace {
 thread_local std::string g_err;
 constexpr uint32_t kRoundSamples = 65536;  // samples per job per round
@@ -44,6 +53,7 @@ class BlockCache {
             std::lock_guard<std::mutex> lk(mu_);
             void *p = take(key);
             if (!p && !pending_[key].empty()) {
+                std::lock_guard<std::mutex> cl(capture_mutex());
                 cudaDeviceSynchronize();
                 for (auto &kv : pending_) {
                     auto &f = ready_[kv.first];
@@ -59,10 +69,14 @@ class BlockCache {
             }
         }
         void *p = nullptr;
-        *err = host ? cudaMallocHost(&p, cls) : cudaMalloc(&p, cls);
+        {
+            std::lock_guard<std::mutex> cl(capture_mutex());
+            *err = host ? cudaMallocHost(&p, cls) : cudaMalloc(&p, cls);
+        }
         if (*err != cudaSuccess) {
             cudaGetLastError();
             release(dev);
+            std::lock_guard<std::mutex> cl(capture_mutex());
             *err = host ? cudaMallocHost(&p, cls) : cudaMalloc(&p, cls);
             if (*err != cudaSuccess) {
                 cudaGetLastError();
@@ -102,6 +116,7 @@ class BlockCache {
     }
     void release(int dev) {
         std::lock_guard<std::mutex> lk(mu_);
+        std::lock_guard<std::mutex> cl(capture_mutex());
         cudaDeviceSynchronize();
         for (auto *m : {&ready_, &pending_})
             for (auto &kv : *m) {
@@ -464,6 +479,7 @@ int Engine::sampler_exec(int block, uint32_t grid, cudaGraphExec_t *out) {
     L.hdr = d_hdr_;
     L.segs = d_segs_;
     cudaGraph_t g = nullptr;
+    std::lock_guard<std::mutex> cl(capture_mutex());
     CK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
     cudaError_t e1 = sampler_round_begin(L, max_segs_, stream_);
     cudaError_t e2 = sampler_launch(L, grid, stream_, block);
@@ -938,13 +954,16 @@ int Job::init() {
     CK(cudaMemset(jc_.sc, 0, sizeof(JobScalars)));
     CK(cudaMemset(jc_.partition, 0, sizeof(int32_t) * n));
     CK(apply_init());
-    CK(cudaDeviceSynchronize());
+    // the set-up above ran on the legacy stream (a whole-device synchronisation
+    // here could meet another thread's graph capture)
+    CK(cudaStreamSynchronize(cudaStreamLegacy));
     return SILVAN_OK;
 }
 
 int Job::capture_apply(cudaStream_t stream) {
     if (apply_graph_) return SILVAN_OK;
     cudaGraph_t g = nullptr;
+    std::lock_guard<std::mutex> cl(capture_mutex());
     CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
     cudaError_t e1 = apply_round(d_state_, rb_.n_touched, stream);
     cudaError_t e2 = cudaStreamEndCapture(stream, &g);

@@ -11,6 +11,7 @@
 #include <array>
 #include <cstdint>
 #include <cstdio>
+#include <mutex>
 #include <string>
 #include <unordered_map>
 #include <vector>
@@ -25,6 +26,7 @@
 namespace silvan {
 
 void set_error(const std::string &msg);
+const char *last_error_cstr();  // this thread's last message
 int cuda_status(cudaError_t e, const char *what);
 double now_seconds();
 
@@ -33,6 +35,10 @@ double now_seconds();
 // DeviceGraph, Engine or Job frees must come from here.
 int device_alloc(void **p, size_t bytes);
 void device_free(void *p);
+
+// Serialises CUDA-graph captures with whole-device synchronisations and
+// allocations made by other threads.
+std::mutex &capture_mutex();
 
 struct DeviceGraph {
     // metadata (always set once uploaded)

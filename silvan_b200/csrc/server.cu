@@ -47,6 +47,7 @@ struct ServerRequest {
     std::vector<double> estimates;
     std::vector<uint32_t> topk_nodes;
     std::vector<double> topk_values;
+    std::string error;  // message of a failed request (set on the thread that failed it)
 };
 
 struct Server {
@@ -218,6 +219,7 @@ struct Server {
 
     // Completes a request: keeps its outputs on the host, frees its device state.
     void finish(ServerRequest *r, int rc) {
+        if (rc != SILVAN_OK) r->error = last_error_cstr();
         const double t_fin = now_seconds();
         struct Acc {
             Server *s;
@@ -326,6 +328,7 @@ int server_poll(Server *s, uint64_t id, int32_t *state, silvan_result_t *res, do
         if (latency) *latency = r->t_done - r->t_submit;
         if (queue_s) *queue_s = r->t_admit - r->t_submit;
     }
+    if (r->state < 0) set_error(r->error);
     return SILVAN_OK;
 }
 
@@ -344,7 +347,9 @@ int server_wait(Server *s, uint64_t id, double timeout_s) {
         set_error("request still running");
         return SILVAN_E_TIMEOUT;
     }
-    return r->state == SILVAN_REQ_DONE ? SILVAN_OK : r->state;
+    if (r->state == SILVAN_REQ_DONE) return SILVAN_OK;
+    set_error(r->error);
+    return r->state;
 }
 
 int server_estimates(Server *s, uint64_t id, double *out, uint32_t n, uint32_t *topk_nodes,

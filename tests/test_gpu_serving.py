@@ -80,3 +80,31 @@ def test_submit_from_threads(sb, small_graphs):
             assert srv.wait(rid, 300)["num_samples"] > 0
     finally:
         srv.close()
+
+
+def test_mixed_stream_all_succeed(sb):
+    """Requests of different sizes and modes arriving back to back: the
+    uploader thread admits and uploads while the round thread captures and
+    launches; every request must finish with its stand-alone result."""
+    graphs = [sb.HostGraph.from_pairs(sb.rmat(s, 16, 70 + s, bool(s % 2)), bool(s % 2))
+              for s in (11, 12, 13, 14, 15, 16)]
+    reqs = []
+    for i in range(18):
+        hg = graphs[i % len(graphs)]
+        k = 5 if i % 5 == 0 else 0
+        eps = 0.1 if k else 0.02
+        reqs.append((hg, eps, k, 300 + i))
+    srv = sb.Server(1 << 16)
+    try:
+        ids = [srv.submit(hg, eps, 0.1, k=k, seed=seed) for hg, eps, k, seed in reqs]
+        outs = []
+        for rid, (hg, eps, k, seed) in zip(ids, reqs):
+            res = srv.wait(rid, 600)
+            outs.append((res, srv.estimates(rid, hg.info().n)))
+    finally:
+        srv.close()
+    for (hg, eps, k, seed), (res, est) in zip(reqs[:6], outs[:6]):
+        job = sb.Probabilistic(sb.Graph.from_host(hg), eps, 0.1, k=k, seed=seed)
+        alone = job.run()
+        assert res["num_samples"] == alone["num_samples"]
+        np.testing.assert_array_equal(est, job.get_centrality())
