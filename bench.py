@@ -380,17 +380,6 @@ def run_multi(args, cfg):
             results.extend(res)
             del jobs
     t = sum(times)
-    # the same jobs one after another (each with the whole GPU), for contrast
-    seq_t, seq_samples = 0.0, 0
-    for i, g in enumerate(graphs):
-        job = sb.Probabilistic(g, cfg["eps"], cfg["delta"], seed=1000 + i, block=args.block)
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        r = job.run()
-        torch.cuda.synchronize()
-        seq_t += time.perf_counter() - t0
-        seq_samples += r["first_pass_samples"] + r["num_samples"]
-        del job
     # e2e: upload of every CSR from pinned host memory, the batched run and
     # the read-back of every estimate, per step
     keep = []
@@ -409,6 +398,19 @@ def run_multi(args, cfg):
         e2e_t += time.perf_counter() - t0
         e2e_samples += sum(r["first_pass_samples"] + r["num_samples"] for r in res)
         del jobs, gs
+    # the same jobs one after another (each with the whole GPU), for contrast
+    seq_t, seq_samples = 0.0, 0
+    # largest graph first, so that every job runs on the engine sized for it
+    for i in sorted(range(len(graphs)), key=lambda i: -csrs[i].n):
+        g = graphs[i]
+        job = sb.Probabilistic(g, cfg["eps"], cfg["delta"], seed=1000 + i, block=args.block)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = job.run()
+        torch.cuda.synchronize()
+        seq_t += time.perf_counter() - t0
+        seq_samples += r["first_pass_samples"] + r["num_samples"]
+        del job
     cpu = None
     if not args.no_cpu_baseline:
         lib = refbench_lib()

@@ -678,10 +678,8 @@ int Engine::round(const std::vector<Job *> &jobs, const std::vector<JobRequest> 
         if (h_hdr_->total > 0 && clock_khz_ > 0) {
             const double cta_ms = (double)h_hdr_->cycles / clock_khz_ / h_hdr_->total;
             const double tail_ms = (double)h_hdr_->max_cycles / clock_khz_;
-            last_cta_ms_ = cta_ms;
-            last_tail_ms_ = tail_ms;
-            last_launch_ms_ = ms;
-            last_grid_ = grid;
+            for (uint32_t i : idx)
+                last_[jobs[i]->graph()->tune_class()] = LastLaunch{cta_ms, tail_ms, ms, grid};
             for (uint32_t i : idx) {
                 BlockStats &st = stats_[jobs[i]->graph()->tune_class()][bi];
                 st.cta_ms = st.rounds ? 0.5 * (st.cta_ms + cta_ms) : cta_ms;
@@ -714,13 +712,16 @@ int Engine::round(const std::vector<Job *> &jobs, const std::vector<JobRequest> 
     return SILVAN_OK;
 }
 
-uint32_t Engine::free_samples(bool tail_only) const {
+uint32_t Engine::free_samples(const DeviceGraph *G, bool tail_only) const {
     // the samples the other slots draw while the slowest sample runs, or
     // while the whole last launch ran (a throughput-bound launch feeds its own
     // length back, so that estimate needs a cap from the caller)
-    const double t = tail_only ? last_tail_ms_ : last_launch_ms_;
-    if (last_cta_ms_ <= 0 || t <= 0) return 0;
-    const double f = t * last_grid_ / last_cta_ms_;
+    auto it = last_.find(G->tune_class());
+    if (it == last_.end()) return 0;
+    const LastLaunch &l = it->second;
+    const double t = tail_only ? l.tail_ms : l.launch_ms;
+    if (l.cta_ms <= 0 || t <= 0) return 0;
+    const double f = t * l.grid / l.cta_ms;
     return (uint32_t)std::min<double>(f, (double)kRoundSamples);
 }
 
@@ -1775,7 +1776,7 @@ int Job::run(silvan_result_t *res, FILE *sink) {
     std::vector<Job *> jobs{this};
     std::vector<JobRequest> reqs(1);
     std::vector<uint64_t> nrec;
-    set_lookahead(own_engine_->free_samples(true), own_engine_->free_samples(false));
+    set_lookahead(own_engine_->free_samples(g_, true), own_engine_->free_samples(g_, false));
     while (!done()) {
         if (!next_request(reqs[0])) {
             set_error("sample index space exhausted");
@@ -1787,7 +1788,7 @@ int Job::run(silvan_result_t *res, FILE *sink) {
             error_ = rc;
             return rc;
         }
-        set_lookahead(own_engine_->free_samples(true), own_engine_->free_samples(false));
+        set_lookahead(own_engine_->free_samples(g_, true), own_engine_->free_samples(g_, false));
     }
     return finish(res);
 }
@@ -1809,7 +1810,7 @@ int Job::step(uint32_t rounds, silvan_status_t *st, FILE *sink) {
         own_engine_->reset_timers();
         launches = 0;
         RK(begin(sink, own_engine_->stream()));
-        set_lookahead(own_engine_->free_samples(true), own_engine_->free_samples(false));
+        set_lookahead(own_engine_->free_samples(g_, true), own_engine_->free_samples(g_, false));
     }
     std::vector<Job *> jobs{this};
     std::vector<JobRequest> reqs(1);
@@ -1825,7 +1826,7 @@ int Job::step(uint32_t rounds, silvan_status_t *st, FILE *sink) {
             error_ = rc;
             return rc;
         }
-        set_lookahead(own_engine_->free_samples(true), own_engine_->free_samples(false));
+        set_lookahead(own_engine_->free_samples(g_, true), own_engine_->free_samples(g_, false));
     }
     if (st) {
         JobScalars sc{};
@@ -1885,7 +1886,8 @@ int run_batched(const std::vector<Job *> &jobs, uint64_t mem_budget, silvan_resu
         for (size_t i = 0; i < act.size(); i++) RK(act[i]->on_drawn(reqs[i], nrec[i]));
         const size_t na = std::max<size_t>(1, act.size());
         for (Job *j : act)
-            j->set_lookahead(eng.free_samples(true) / na, eng.free_samples(false) / na);
+            j->set_lookahead(eng.free_samples(j->graph(), true) / na,
+                             eng.free_samples(j->graph(), false) / na);
     }
     for (size_t i = 0; i < jobs.size(); i++) RK(jobs[i]->finish(&results[i]));
     return SILVAN_OK;

@@ -124,7 +124,8 @@ class Engine {
     // samples that one more launch could draw for free: a launch lasts at
     // least as long as its slowest sample, during which the other slots keep
     // drawing (0 until a launch has been measured)
-    uint32_t free_samples(bool tail_only) const;
+    // measured on the last launch that drew samples of G's class of graphs
+    uint32_t free_samples(const DeviceGraph *G, bool tail_only) const;
     uint64_t launches() const { return launches_; }
     float sample_ms() const { return sample_ms_; }
     void reset_timers() {
@@ -177,10 +178,13 @@ class Engine {
     float sample_ms_ = 0;
     uint64_t launches_ = 0;
     double clock_khz_ = 0;
-    double last_cta_ms_ = 0;     // CTA ms per sample of the last launch
-    double last_tail_ms_ = 0;    // its slowest sample
-    double last_launch_ms_ = 0;
-    uint32_t last_grid_ = 0;
+    struct LastLaunch {
+        double cta_ms = 0;     // CTA ms per sample
+        double tail_ms = 0;    // the slowest sample
+        double launch_ms = 0;
+        uint32_t grid = 0;
+    };
+    std::unordered_map<uint64_t, LastLaunch> last_;  // by tune_class()
 };
 
 class Job {

@@ -149,13 +149,13 @@ struct Server {
                 continue;
             }
             const size_t na = std::max<size_t>(1, owners.size());
-            const uint32_t la_tail = eng.free_samples(true) / na;
-            const uint32_t la = eng.free_samples(false) / na;
+
             for (size_t i = 0; i < owners.size(); i++) {
                 ServerRequest *r = owners[i];
                 const double t_commit = now_seconds();
                 int e = r->job->on_drawn(reqs[i], nrec[i]);
-                r->job->set_lookahead(la_tail, la);
+                r->job->set_lookahead(eng.free_samples(r->graph.get(), true) / na,
+                                      eng.free_samples(r->graph.get(), false) / na);
                 account(2, t_commit);
                 if (e != SILVAN_OK) finish(r, e);
                 else if (r->job->done()) finish(r, SILVAN_OK);
