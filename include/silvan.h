@@ -79,7 +79,10 @@ typedef struct {
     uint32_t block;      /* threads per sampler slot: 0 = autotuned per graph
                             and round, else 128, 256, 512 or 1024            */
     uint32_t backtrack;  /* SILVAN_BACKTRACK_*                               */
-    uint32_t reserved;
+    uint32_t assist_items; /* BFS levels of at least this many adjacency
+                            entries are expanded by several sampler CTAs
+                            together (same results): 0 = default (32 x the
+                            CTA size: eight tiles), 0xffffffff = never      */
 } silvan_params_t;
 
 /* Predecessor choice of the random backtrack.  REFERENCE is the rule of
@@ -129,6 +132,10 @@ typedef struct {
     uint32_t sampler_launches;   /* persistent sampler launches (own engine) */
     uint32_t sampler_block;      /* CTA size that drew most samples          */
     uint64_t samples_drawn;      /* samples drawn, speculative ones included */
+    uint32_t assisted_levels;    /* BFS levels expanded by several CTAs (own
+                                    engine; see silvan_params_t::assist_items) */
+    uint32_t pad0;
+    uint64_t helper_tiles;       /* tiles of those levels done by helpers    */
 } silvan_result_t;
 
 /* ---- graphs (reference: Graph, silvan/src/Graph.cpp) ------------------- */

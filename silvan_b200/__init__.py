@@ -60,7 +60,7 @@ class Params(C.Structure):
                 ("form", C.c_int32), ("a", C.c_double), ("seed", C.c_uint64),
                 ("verbose", C.c_double), ("np_cap", C.c_uint32), ("slots", C.c_uint32),
                 ("threads", C.c_uint32), ("block", C.c_uint32),
-                ("backtrack", C.c_uint32), ("reserved", C.c_uint32)]
+                ("backtrack", C.c_uint32), ("assist_items", C.c_uint32)]
 
 
 class Result(C.Structure):
@@ -80,7 +80,8 @@ class Result(C.Structure):
                 ("time_device_s", C.c_double), ("ball_nodes", C.c_uint64),
                 ("pred_entries", C.c_uint64), ("kernel_launches", C.c_uint64),
                 ("sampler_launches", C.c_uint32), ("sampler_block", C.c_uint32),
-                ("samples_drawn", C.c_uint64)]
+                ("samples_drawn", C.c_uint64), ("assisted_levels", C.c_uint32),
+                ("pad0", C.c_uint32), ("helper_tiles", C.c_uint64)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}
@@ -372,7 +373,7 @@ class Probabilistic:
 
     def __init__(self, graph: Graph, eps, delta, k=0, alpha=2.3, alpha_given=False, a=2.0,
                  m_hat=True, seed=42, form="batched", verbose=0.0, np_cap=0, slots=0,
-                 threads=1, block=0, backtrack="reference"):
+                 threads=1, block=0, backtrack="reference", assist_items=0):
         lib = load()
         p = Params()
         lib.silvan_params_default(C.byref(p))
@@ -381,6 +382,7 @@ class Probabilistic:
         p.m_hat, p.seed, p.verbose = int(m_hat), seed, verbose
         p.form = FORM_PLAIN if form == "plain" else FORM_BATCHED
         p.np_cap, p.slots, p.threads, p.block = np_cap, slots, threads, block
+        p.assist_items = assist_items
         p.backtrack = {"reference": BACKTRACK_REFERENCE,
                        "sigma": BACKTRACK_SIGMA_WEIGHTED}[backtrack]
         self.graph = graph

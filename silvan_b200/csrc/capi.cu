@@ -91,7 +91,7 @@ void silvan_params_default(silvan_params_t *p) {
     p->threads = 1;
     p->block = 0;
     p->backtrack = SILVAN_BACKTRACK_REFERENCE;
-    p->reserved = 0;
+    p->assist_items = 0;
 }
 
 const char *silvan_last_error(void) { return last_error_cstr(); }

@@ -5,6 +5,7 @@
 #include <atomic>
 #include <chrono>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <iomanip>
 #include <map>
@@ -94,6 +95,16 @@ class BlockCache {
         if (it == live_.end()) return;
         pending_[it->second].push_back(p);
         live_.erase(it);
+    }
+
+    // Device bytes held by freed blocks of device dev kept for reuse.
+    uint64_t idle_bytes(int dev) {
+        std::lock_guard<std::mutex> lk(mu_);
+        uint64_t b = 0;
+        for (auto *m : {&ready_, &pending_})
+            for (auto &kv : *m)
+                if (kv.first.first == dev) b += (uint64_t)kv.first.second * kv.second.size();
+        return b;
     }
 
   private:
@@ -404,6 +415,7 @@ Engine::~Engine() {
     for (auto &e : ev_)
         if (e) cudaEventDestroy(e);
     slots_.free_all();
+    device_free(board_mem_);
     if (stream_) cudaStreamDestroy(stream_);
 }
 
@@ -430,13 +442,20 @@ int Engine::init(uint64_t n_max, uint32_t slots, uint64_t mem_budget) {
     }
     if (slots == 0) slots = std::max<uint32_t>(most, 1);
     if (mem_budget == 0) {
+        // half of the free memory, counting the blocks this process freed
+        // and keeps for reuse (an engine created after another one would
+        // otherwise see half of the previous budget, and so on)
         size_t fr = 0, tot = 0;
+        int dev = 0;
+        CK(cudaGetDevice(&dev));
         CK(cudaMemGetInfo(&fr, &tot));
-        mem_budget = fr / 2;
+        mem_budget = (fr + block_cache().idle_bytes(dev)) / 2;
     }
     const uint64_t fit = mem_budget / std::max<uint64_t>(SlotPool::bytes_per_slot(n_max), 1);
     if (fit < slots) slots = (uint32_t)std::max<uint64_t>(fit, 1);
     RK(slots_.alloc(slots, n_max, stream_));
+    RK(device_alloc(&board_mem_, assist_board_bytes(n_max)));
+    CK(assist_board_init(&board_, board_mem_, n_max, stream_));
     for (int b = 0; b < kNB; b++) max_grid_[b] = std::min(resident[b], slots);
     RK(dmalloc(&d_hdr_, 1));
     RK(hmalloc(&h_hdr_, 1));
@@ -478,6 +497,7 @@ int Engine::sampler_exec(int block, uint32_t grid, cudaGraphExec_t *out) {
                          slots_.meet, slots_.meet_pre, slots_.n};
     L.hdr = d_hdr_;
     L.segs = d_segs_;
+    L.assist = board_;
     cudaGraph_t g = nullptr;
     std::lock_guard<std::mutex> cl(capture_mutex());
     CK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
@@ -616,6 +636,10 @@ int Engine::round(const std::vector<Job *> &jobs, const std::vector<JobRequest> 
         S.alpha = r.alpha;
         S.np_cap = job->params().np_cap;
         S.weighted = job->params().backtrack == SILVAN_BACKTRACK_SIGMA_WEIGHTED ? 1 : 0;
+        {
+            const uint32_t ai = job->params().assist_items;
+            S.assist_items = ai == 0u ? kAssistItemsAuto : (ai == 0xffffffffu ? 0u : ai);
+        }
         S.first_sample = r.first_global;
         S.count = r.count;
         S.base = base;
@@ -672,6 +696,8 @@ int Engine::round(const std::vector<Job *> &jobs, const std::vector<JobRequest> 
         cudaEventElapsedTime(&ms, ev_[0], ev_[1]);
         sample_ms_ += ms;
         block_samples_[bi] += total;
+        assisted_levels_ += h_hdr_->assisted;
+        helper_tiles_ += h_hdr_->helper_tiles;
         // cost model of the CTA-size choice and of speculative draws: a launch
         // lasts about as long as its slowest sample, so the samples that fit
         // into that time on the other slots cost (almost) nothing extra
@@ -679,11 +705,15 @@ int Engine::round(const std::vector<Job *> &jobs, const std::vector<JobRequest> 
             const double cta_ms = (double)h_hdr_->cycles / clock_khz_ / h_hdr_->total;
             const double tail_ms = (double)h_hdr_->max_cycles / clock_khz_;
             for (uint32_t i : idx)
-                last_[jobs[i]->graph()->tune_class()] = LastLaunch{cta_ms, tail_ms, ms, grid};
+                last_[jobs[i]->graph()->tune_class()] = LastLaunch{cta_ms, tail_ms, ms, grid, total};
             for (uint32_t i : idx) {
+                // the slowest sample of a launch grows with the launch's size
+                // and is rare: the estimate follows a longer tail at once and
+                // a shorter one slowly
                 BlockStats &st = stats_[jobs[i]->graph()->tune_class()][bi];
                 st.cta_ms = st.rounds ? 0.5 * (st.cta_ms + cta_ms) : cta_ms;
-                st.tail_ms = st.rounds ? 0.5 * (st.tail_ms + tail_ms) : tail_ms;
+                st.tail_ms = (!st.rounds || tail_ms > st.tail_ms) ? tail_ms
+                                                                  : 0.75 * st.tail_ms + 0.25 * tail_ms;
                 st.rounds++;
             }
         }
@@ -721,7 +751,11 @@ uint32_t Engine::free_samples(const DeviceGraph *G, bool tail_only) const {
     const LastLaunch &l = it->second;
     const double t = tail_only ? l.tail_ms : l.launch_ms;
     if (l.cta_ms <= 0 || t <= 0) return 0;
-    const double f = t * l.grid / l.cta_ms;
+    double f = t * l.grid / l.cta_ms;
+    // a launch longer than its work (a long tail) predicts many free samples;
+    // the next launch may not have that tail, so the estimate grows by at
+    // most a factor of two per launch
+    if (!tail_only) f = std::min(f, 2.0 * l.samples);
     return (uint32_t)std::min<double>(f, (double)kRoundSamples);
 }
 
@@ -1338,6 +1372,10 @@ int Job::stop_check(bool &stop) {
             out << "MCRADE STOPS at sample size " << pass_samples_ << "\n";
         } else {
             out << "   mcrade eps " << sup << "\n";
+            // the bound shrinks about as 1 / sqrt(samples): the sample size
+            // at which it reaches eps sizes the draws ahead of the stop
+            const double r = sup / p_.eps;
+            if (r > 1 && r < 1e3) predicted_stop_ = (uint64_t)((double)pass_samples_ * r * r * 1.02);
         }
         out_ += out.str();
         return SILVAN_OK;
@@ -1418,7 +1456,21 @@ bool Job::next_request(JobRequest &r) {
         // the ones beyond the final stop are discarded.  In absolute mode the
         // first pass has a fixed length, and the samples drawn beyond it are
         // the second pass's first ones when the second pass keeps alpha.
-        cnt = std::max<uint64_t>(cnt, phase_ == kPass2 ? lookahead_ : lookahead_tail_);
+        // in the first pass, at most four times its length: a long tail
+        // would otherwise ask for a launch whose size favours long tails
+        uint64_t ahead = phase_ == kPass2 ? lookahead_
+                                          : std::min<uint64_t>(lookahead_tail_, 4 * target_);
+        if (phase_ == kPass2 && predicted_stop_ > pass_samples_) {
+            // absolute mode after a failed check: up to the schedule point at
+            // or after the predicted stop (at most 4x the samples so far)
+            uint64_t ns = std::max<uint64_t>(next_stop_, 1);
+            const uint64_t want = std::min<uint64_t>(predicted_stop_, 5 * pass_samples_);
+            while (ns < want && (double)ns < last_stop_)
+                ns = std::max<uint64_t>(ns + 1, (uint64_t)(ns * 1.2));
+            const uint64_t b = (uint64_t)kBlock * ((ns + kBlock - 1) / kBlock);
+            ahead = std::max<uint64_t>(lookahead_tail_, b > pass_samples_ ? b - pass_samples_ : 0);
+        }
+        cnt = std::max<uint64_t>(cnt, ahead);
         if (phase_ == kPass2 && p_.m_hat) {
             // the omega cap only decreases, so the run never goes beyond it
             const uint64_t cap = (uint64_t)kBlock * (uint64_t)ceil(omega_ / kBlock);
@@ -1751,6 +1803,8 @@ int Job::evaluate() {
     res.sampler_launches = own_engine_ ? own_engine_->sampler_launches() : 0;
     res.sampler_block = own_engine_ ? own_engine_->main_block() : 0;
     res.samples_drawn = drawn_;
+    res.assisted_levels = own_engine_ ? own_engine_->assisted_levels() : 0;
+    res.helper_tiles = own_engine_ ? own_engine_->helper_tiles() : 0;
     phase_ = kDone;
     return SILVAN_OK;
 }

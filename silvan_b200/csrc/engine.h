@@ -132,9 +132,13 @@ class Engine {
         sample_ms_ = 0;
         launches_ = 0;
         sampler_launches_ = 0;
+        assisted_levels_ = 0;
+        helper_tiles_ = 0;
         block_samples_.fill(0);
     }
     uint32_t sampler_launches() const { return sampler_launches_; }
+    uint32_t assisted_levels() const { return assisted_levels_; }
+    uint64_t helper_tiles() const { return helper_tiles_; }
     // Shortens the requests of a multi-job round so that the round's
     // predicted CTA time fits `round_ms` on the resident slots: jobs that
     // need little get all of it, the rest share what is left evenly (every
@@ -164,6 +168,8 @@ class Engine {
     int sampler_exec(int block, uint32_t grid, cudaGraphExec_t *out);
     void drop_execs();
     SlotPool slots_;
+    void *board_mem_ = nullptr;  // help board of the sampler launches
+    AssistBoard board_{};
     cudaStream_t stream_ = nullptr;
     RoundHeader *d_hdr_ = nullptr, *h_hdr_ = nullptr;
     SegDesc *d_segs_ = nullptr, *h_segs_ = nullptr;
@@ -174,6 +180,8 @@ class Engine {
     std::unordered_map<uint64_t, std::array<BlockStats, kNB>> stats_;  // by tune_class()
     std::array<uint64_t, kNB> block_samples_{};
     uint32_t sampler_launches_ = 0;
+    uint32_t assisted_levels_ = 0;  // BFS levels expanded with the help board
+    uint64_t helper_tiles_ = 0;     // tiles of those levels done by helping CTAs
     cudaEvent_t ev_[4] = {nullptr, nullptr, nullptr, nullptr};
     float sample_ms_ = 0;
     uint64_t launches_ = 0;
@@ -183,6 +191,7 @@ class Engine {
         double tail_ms = 0;    // the slowest sample
         double launch_ms = 0;
         uint32_t grid = 0;
+        uint32_t samples = 0;  // drawn by the launch
     };
     std::unordered_map<uint64_t, LastLaunch> last_;  // by tune_class()
 };
@@ -290,6 +299,7 @@ class Job {
     uint64_t base_global_ = 0;   // global index of the pass's first sample
     uint32_t lookahead_ = 0;     // pass 2: samples drawn ahead of the next point
     uint32_t lookahead_tail_ = 0;  // pass 1 (absolute mode): samples drawn beyond it
+    uint64_t predicted_stop_ = 0;  // pass 2 (absolute mode): sample size of the likely stop
     float commit_ms_ = 0;
     uint64_t drawn_ = 0;         // samples drawn over both passes
     cudaEvent_t ev_commit_[2] = {nullptr, nullptr};

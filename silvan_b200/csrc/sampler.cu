@@ -23,7 +23,9 @@
 //            block scan), which appends new nodes to the queue and meeting
 //            edges to the list in the reference order.
 // A later tile can never lower a node's minimum below an earlier tile's g, so
-// each tile is final once its own phase 1 is done.
+// each tile is final once its own phase 1 is done.  A wide level may instead
+// be expanded by several CTAs, tile by tile with the same numbering (the help
+// board, below).
 //
 // The backtrack needs pred(y)[t] with t = min(r mod sigma(y), |pred(y)| - 1)
 // (Sp_sampler.cpp:241-265: the walk adds n_paths[v] == 1 per entry).  t == 0
@@ -82,6 +84,13 @@ struct SamplerSmem {
     uint32_t lvl_lo[2][kMaxLevels];
     uint32_t lvl_hi[2][kMaxLevels];
     SegDesc seg;  // the segment of the sample in flight
+    // help board
+    AssistLevel lvl;   // the level this CTA expands with others
+    int32_t a_entry;   // entry owned or helped; -1 none, -2 leave, -3 a sample
+    uint32_t a_state;  // state of the owned entry while it is set up
+    uint32_t a_tile;   // the tile this CTA took
+    uint32_t a_ok;     // the tile's waits ended
+    uint32_t a_drained, a_polls, a_nap;  // no sample left; board polls since; next nap (ns)
 };
 
 __device__ __forceinline__ uint32_t lanemask_lt() {
@@ -498,6 +507,607 @@ __device__ void expand_level(const SegDesc &A, SamplerSmem<BLOCK> &s, NodeRec *r
     // the caller's thread 0 consumes sum_new before its next barrier
 }
 
+// ---------------------------------------------------------------------------
+// Wide levels expanded by several CTAs (the help board)
+//
+// A launch lasts about as long as its slowest sample, and the slowest samples
+// spend most of their time in one or two wide levels (hub rows, ~10^5
+// entries) on one CTA.  Such a level is posted on the board instead: its
+// owner writes the frontier's item prefix and a table of tiles (at most kTile
+// items inside one chunk of kChunk frontier nodes), and every CTA that joins,
+// the owner included, takes the next tile in order and runs expand_level's
+// two phases on it.  Two decoupled look-backs over the tiles stand in for the
+// one-CTA tile order:
+//   * after its phase 1 a tile waits until the phase 1 of every earlier tile
+//     is done (a later tile cannot lower a minimum below its own items, so
+//     its joining hits are then final);
+//   * its joins and meeting edges go to the offsets summed over the earlier
+//     tiles, in item order within the tile.
+// The items, keys, joins and append order are those of expand_level, so the
+// level's result is bit-identical.  Tiles are taken in order and no tile
+// waits for a later one, so every wait ends; each is bounded all the same: a
+// wait that gives up marks the level failed (the sample reports
+// SILVAN_E_TIMEOUT) and the tile skips its writes.
+// ---------------------------------------------------------------------------
+constexpr uint32_t kAssistSpin = 1u << 20;   // polls of a bounded wait (>= 0.1 s)
+constexpr uint32_t kAssistPolls = 1u << 18;  // board polls of a CTA without samples
+constexpr unsigned long long kCntMask = (1ull << 31) - 1u;
+
+__device__ __forceinline__ uint32_t ld_acquire_u32(const uint32_t *p) {
+    uint32_t v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void st_release_u32(uint32_t *p, uint32_t v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long *p) {
+    unsigned long long v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void st_release_u64(unsigned long long *p, unsigned long long v) {
+    asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// Look-back word of a tile's append counts: state (1 own counts, 2 inclusive
+// prefix), joins, meeting edges (each saturated to 31 bits).
+__device__ __forceinline__ unsigned long long cnt_word(uint32_t state, unsigned long long j,
+                                                       unsigned long long m) {
+    return ((unsigned long long)state << 62) | (min(j, kCntMask) << 31) | min(m, kCntMask);
+}
+
+// Thread 0: waits until *p == 0 (false: gave up).
+__device__ bool wait_zero(const uint32_t *p) {
+    for (uint32_t i = 0; i < kAssistSpin; i++) {
+        if (ld_acquire_u32(p) == 0u) return true;
+        __nanosleep(128);
+    }
+    return false;
+}
+
+// Thread 0: waits until *p >= v (false: gave up).
+__device__ bool wait_at_least(const uint32_t *p, uint32_t v) {
+    for (uint32_t i = 0; i < kAssistSpin; i++) {
+        if (ld_acquire_u32(p) >= v) return true;
+        __nanosleep(128);
+    }
+    return false;
+}
+
+// Warp 0: waits until the phase 1 of every tile before t is done.  hit_flag
+// of a tile is 1 once its own hits are recorded and 2 once those of every
+// tile up to it are; the warp reads 32 predecessors at a time.
+__device__ bool lookback_hits(const uint32_t *hit_flag, uint32_t t) {
+    const uint32_t lane = threadIdx.x & 31;
+    uint32_t j = t;
+    for (uint32_t spin = 0; spin < kAssistSpin;) {
+        if (j == 0) return true;
+        const uint32_t f = lane < j ? ld_acquire_u32(&hit_flag[j - 1 - lane]) : 2u;
+        const uint32_t m2 = __ballot_sync(0xffffffffu, f == 2u);
+        const uint32_t m0 = __ballot_sync(0xffffffffu, f == 0u);
+        if (m2) {
+            if ((m0 & ((m2 & (0u - m2)) - 1u)) == 0u) return true;
+        } else if (m0 == 0u) {
+            j -= 32u;  // j > 32 here: lanes at or past j read as 2
+            continue;
+        }
+        __nanosleep(64);
+        spin++;
+    }
+    return false;
+}
+
+// Warp 0: sums of the joins and meeting edges of the tiles before t (the
+// decoupled look-back of a single-pass scan).  The same in every lane.
+__device__ bool lookback_counts(const unsigned long long *cnt_flag, uint32_t t,
+                                unsigned long long &ej, unsigned long long &em) {
+    const uint32_t lane = threadIdx.x & 31;
+    uint32_t j = t;
+    ej = em = 0;
+    for (uint32_t spin = 0; spin < kAssistSpin;) {
+        if (j == 0) return true;
+        const unsigned long long w =
+            lane < j ? ld_acquire_u64(&cnt_flag[j - 1 - lane]) : cnt_word(2u, 0, 0);
+        const uint32_t st = (uint32_t)(w >> 62);
+        const uint32_t m2 = __ballot_sync(0xffffffffu, st == 2u);
+        const uint32_t m0 = __ballot_sync(0xffffffffu, st == 0u);
+        uint32_t take = 0xffffffffu;
+        if (m2) {
+            const uint32_t first = m2 & (0u - m2);
+            take = first | (first - 1u);
+        }
+        if (m0 & take) {  // a tile on the way has not counted yet
+            __nanosleep(64);
+            spin++;
+            continue;
+        }
+        unsigned long long vj = ((take >> lane) & 1u) ? (w >> 31) & kCntMask : 0ull;
+        unsigned long long vm = ((take >> lane) & 1u) ? w & kCntMask : 0ull;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            vj += __shfl_xor_sync(0xffffffffu, vj, o);
+            vm += __shfl_xor_sync(0xffffffffu, vm, o);
+        }
+        ej += vj;
+        em += vm;
+        if (m2) return true;
+        j -= 32u;
+    }
+    return false;
+}
+
+// Thread 0: copies an open entry's level description (through L2: another
+// SM wrote it).
+__device__ void load_level(AssistLevel &dst, const AssistLevel *src) {
+    const uint32_t *a = reinterpret_cast<const uint32_t *>(src);
+    uint32_t *b = reinterpret_cast<uint32_t *>(&dst);
+    for (uint32_t i = 0; i < sizeof(AssistLevel) / 4; i++) b[i] = __ldcg(a + i);
+}
+
+// Thread 0: takes a free entry for this CTA's level (-1: none free).
+__device__ int32_t acquire_entry(const AssistBoard &B, uint32_t from, uint32_t &st_out) {
+    for (uint32_t i = 0; i < kAssistEntries; i++) {
+        const uint32_t e = (from + i) % kAssistEntries;
+        const uint32_t st = ld_acquire_u32(&B.entries[e].state);
+        if ((st & 3u) != 0u) continue;
+        if (atomicCAS(&B.entries[e].state, st, st | 1u) == st) {
+            st_out = st | 1u;
+            return (int32_t)e;
+        }
+    }
+    return -1;
+}
+
+// Thread 0: enters an open entry with tiles left, copying its level into
+// s.lvl (-1: none).  The entry count `inside` is raised before the state is
+// read again, so the owner either sees this helper or the helper sees the
+// entry closing and leaves.
+template <int BLOCK>
+__device__ __noinline__ int32_t join_entry(const SamplerLaunch &L, SamplerSmem<BLOCK> &s,
+                                           uint32_t from) {
+    const uint32_t mask = ld_acquire_u32(&L.hdr->open_mask);
+    if (!mask) return -1;
+    for (uint32_t i = 0; i < kAssistEntries; i++) {
+        const uint32_t e = (from + i) % kAssistEntries;
+        if (!(mask & (1u << e))) continue;
+        AssistEntry *E = L.assist.entries + e;
+        const uint32_t st = ld_acquire_u32(&E->state);
+        if ((st & 3u) != 2u) continue;
+        if (ld_acquire_u32(&E->claim) >= ld_acquire_u32(&E->ntiles)) continue;
+        atomicAdd(&E->inside, 1u);
+        __threadfence();
+        if (ld_acquire_u32(&E->state) != st) {
+            atomicSub(&E->inside, 1u);
+            continue;
+        }
+        load_level(s.lvl, &E->lvl);
+        return (int32_t)e;
+    }
+    return -1;
+}
+
+// Thread 0, before a level of the sample in flight: takes a board entry for
+// it when it is wide (-1: expand it alone).  The level's items are the degree
+// sum of its frontier: the side's sum for depth >= 1, the root's degree at 0.
+template <int BLOCK>
+__device__ __forceinline__ int32_t post_level(const SamplerLaunch &L, SamplerSmem<BLOCK> &s,
+                                           bool side_u, uint32_t lo, uint32_t hi,
+                                           uint32_t depth) {
+    const SegDesc &A = s.seg;
+    const uint32_t *doff = side_u ? A.out_off : A.in_off;
+    const uint32_t x0 = side_u ? s.u : s.v;
+    const uint32_t items = depth == 0 ? doff[x0 + 1] - doff[x0] : (side_u ? s.sum_u : s.sum_v);
+    const uint32_t F = hi - lo;
+    const uint32_t thr =
+        A.assist_items == kAssistItemsAuto ? 8u * (uint32_t)Shape<BLOCK>::kTile : A.assist_items;
+    if (items < thr || F > L.assist.node_cap ||
+        (uint64_t)items / Shape<BLOCK>::kTile + F / Shape<BLOCK>::kChunk + 2u > L.assist.tile_cap)
+        return -1;
+    return acquire_entry(L.assist, blockIdx.x, s.a_state);
+}
+
+// Tile t of entry e's level: expand_level's two phases on the tile's items.
+template <int BLOCK>
+__device__ void assist_tile(SamplerSmem<BLOCK> &s, const AssistBoard &B, uint32_t e, uint32_t t) {
+    constexpr int kWarps = Shape<BLOCK>::kWarps;
+    constexpr int kPer = Shape<BLOCK>::kPerThread;
+    const AssistLevel &V = s.lvl;
+    AssistEntry *E = B.entries + e;
+    const uint64_t tb = (uint64_t)e * B.tile_cap;
+    const uint32_t *pre = B.pre + (uint64_t)e * (B.node_cap + 1u);
+    const uint32_t *rs = B.rs + (uint64_t)e * B.node_cap;
+    uint32_t *hit_flag = B.hit_flag + tb;
+    unsigned long long *cnt_flag = B.cnt_flag + tb;
+    const uint4 tl = __ldcg(&B.tiles[tb + t]);
+    const uint32_t l0 = tl.x, ln = tl.y, g0 = tl.z, g1 = tl.w;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    // stage the frontier nodes [l0, l0 + ln) that hold the tile's items
+    {
+        uint32_t xq[kPer];
+#pragma unroll
+        for (int i = 0; i < kPer; i++) {
+            const uint32_t p = threadIdx.x * kPer + i;
+            xq[i] = 0u;
+            if (p < ln) {
+                xq[i] = __ldcg(&V.queue[V.lo + l0 + p]);
+                s.f_off[p] = __ldcg(&rs[l0 + p]);
+                s.f_pre[p] = __ldcg(&pre[l0 + p]);
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < kPer; i++) {
+            const uint32_t p = threadIdx.x * kPer + i;
+            if (p < ln) {
+                s.f_node[p] = xq[i];
+                s.f_sig[p] = __ldcg(&V.rec[xq[i]].sigma);
+            }
+        }
+        if (threadIdx.x == 0) s.f_pre[ln] = __ldcg(&pre[l0 + ln]);
+    }
+    __syncthreads();
+    // ---- phase 1 (as in expand_level) ----------------------------------------
+    uint32_t ys[kItems], xs[kItems], code[kItems], li[kItems];
+#pragma unroll
+    for (int k = 0; k < kItems; k++) {
+        const uint32_t it = g0 + (uint32_t)(k * BLOCK) + threadIdx.x;
+        code[k] = 0;
+        ys[k] = 0;
+        xs[k] = 0;
+        li[k] = 0;
+        if (it < g1) {
+            uint32_t l = 0, h = ln;
+            while (h - l > 1) {
+                const uint32_t mid = (l + h) >> 1;
+                if (s.f_pre[mid] <= it) l = mid;
+                else h = mid;
+            }
+            li[k] = l;
+            xs[k] = s.f_node[l];
+            ys[k] = __ldg(&V.adj[s.f_off[l] + (it - s.f_pre[l])]);
+            code[k] = 3;
+        }
+    }
+    uint32_t sty[kItems];
+#pragma unroll
+    for (int k = 0; k < kItems; k++) sty[k] = code[k] ? __ldcg(&V.rec[ys[k]].st) : 0u;
+    // joins of earlier tiles only turn a state 0 into new_st: the classes
+    // are those of the level's start
+#pragma unroll
+    for (int k = 0; k < kItems; k++) {
+        if (!code[k]) continue;
+        if (sty[k] == 0u || sty[k] == V.new_st) code[k] = 1;
+        else if (st_side(sty[k]) != V.side) code[k] = 2;
+        else code[k] = 0;
+    }
+    uint32_t nh = 0;
+#pragma unroll
+    for (int k = 0; k < kItems; k++) {
+        if (code[k] != 1) continue;
+        const uint32_t it = g0 + (uint32_t)(k * BLOCK) + threadIdx.x;
+        const unsigned long long key = ((unsigned long long)it << 32) | xs[k];
+        NodeRec *r = &V.rec[ys[k]];
+        atomicMin(reinterpret_cast<unsigned long long *>(&r->first), key);
+        atomicMax(reinterpret_cast<unsigned long long *>(&r->last), key);
+        atomicAdd(&r->cnt, 1u);
+        atomicAdd(reinterpret_cast<unsigned long long *>(&r->sigma), s.f_sig[li[k]]);
+        nh++;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) nh += __shfl_xor_sync(0xffffffffu, nh, o);
+    if (lane == 0 && nh) atomicAdd(&E->hits, nh);
+    __syncthreads();
+    if (warp == 0) {
+        if (lane == 0) {
+            __threadfence();
+            st_release_u32(&hit_flag[t], 1u);
+        }
+        __syncwarp();
+        const bool ok = lookback_hits(hit_flag, t);
+        if (lane == 0) {
+            // published even after a failed wait, so that later tiles do not
+            // wait as well (the level is reported failed)
+            st_release_u32(&hit_flag[t], 2u);
+            __threadfence();
+            s.a_ok = ok ? 1u : 0u;
+            if (!ok) atomicExch(&E->err, 1u);
+        }
+    }
+    __syncthreads();
+    // ---- phase 2: joining hits and meeting edges, in item order ---------------
+    unsigned long long fv[kItems];
+    uint32_t dg[kItems];
+#pragma unroll
+    for (int k = 0; k < kItems; k++) {
+        fv[k] = code[k] == 1
+                    ? __ldcg(reinterpret_cast<const unsigned long long *>(&V.rec[ys[k]].first))
+                    : 0ull;
+        dg[k] = code[k] == 1 ? __ldg(&V.off[ys[k] + 1]) - __ldg(&V.off[ys[k]]) : 0u;
+    }
+    uint32_t rnm[kItems];  // rank among the warp's joins (low half) and meeting edges
+#pragma unroll
+    for (int k = 0; k < kItems; k++) {
+        const uint32_t it = g0 + (uint32_t)(k * BLOCK) + threadIdx.x;
+        if (code[k] == 1 && (uint32_t)(fv[k] >> 32) != it) code[k] = 0;
+        const uint32_t bn = __ballot_sync(0xffffffffu, code[k] == 1);
+        const uint32_t bm = __ballot_sync(0xffffffffu, code[k] == 2);
+        rnm[k] = __popc(bn & lanemask_lt()) | (__popc(bm & lanemask_lt()) << 16);
+        if (lane == 0) {
+            s.warp_a[k * kWarps + warp] = __popc(bn);
+            s.warp_b[k * kWarps + warp] = __popc(bm);
+        }
+    }
+    __syncthreads();
+    if (warp == 0) {
+        // offsets over (item slot, warp) as in expand_level, based on the
+        // earlier tiles' sums
+        constexpr int kE = kItems * kWarps;
+        constexpr int kPerLane = (kE + 31) / 32;
+        uint32_t va[kPerLane], vb[kPerLane];
+        uint32_t sa = 0, sb = 0;
+#pragma unroll
+        for (int i = 0; i < kPerLane; i++) {
+            const int x = lane * kPerLane + i;
+            va[i] = x < kE ? s.warp_a[x] : 0u;
+            vb[i] = x < kE ? s.warp_b[x] : 0u;
+            sa += va[i];
+            sb += vb[i];
+        }
+        uint32_t ia = sa, ib = sb;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t ta = __shfl_up_sync(0xffffffffu, ia, o);
+            const uint32_t tb2 = __shfl_up_sync(0xffffffffu, ib, o);
+            if (lane >= o) {
+                ia += ta;
+                ib += tb2;
+            }
+        }
+        const uint32_t aj = __shfl_sync(0xffffffffu, ia, 31);
+        const uint32_t am = __shfl_sync(0xffffffffu, ib, 31);
+        if (lane == 0) st_release_u64(&cnt_flag[t], cnt_word(t == 0 ? 2u : 1u, aj, am));
+        unsigned long long ej = 0, em = 0;
+        bool ok = true;
+        if (t > 0) {
+            __syncwarp();
+            ok = lookback_counts(cnt_flag, t, ej, em);
+            if (lane == 0) st_release_u64(&cnt_flag[t], cnt_word(2u, ej + aj, em + am));
+        }
+        ok = ok && s.a_ok != 0u;
+        if (lane == 0) {
+            atomicAdd(&E->joins, aj);
+            atomicAdd(&E->meets, am);
+            if (!ok) atomicExch(&E->err, 1u);
+        }
+        const unsigned long long qb = (unsigned long long)V.qbase + ej;
+        const unsigned long long mb = (unsigned long long)V.mbase + em;
+        uint32_t ea = (uint32_t)min(qb, 0xffffffffull) + ia - sa;
+        uint32_t eb = (uint32_t)min(mb, (unsigned long long)kMeetCap) + ib - sb;
+        __syncwarp();
+#pragma unroll
+        for (int i = 0; i < kPerLane; i++) {
+            const int x = lane * kPerLane + i;
+            if (x < kE) {
+                s.warp_a[x] = ea;
+                s.warp_b[x] = eb;
+            }
+            ea += va[i];
+            eb += vb[i];
+        }
+        if (lane == 0) s.a_ok = ok ? 1u : 0u;
+    }
+    __syncthreads();
+    uint32_t sum = 0;
+    if (s.a_ok) {
+#pragma unroll
+        for (int k = 0; k < kItems; k++) {
+            if (code[k] == 1) {
+                const uint32_t y = ys[k];
+                V.queue[s.warp_a[k * kWarps + warp] + (rnm[k] & 0xffffu)] = y;
+                V.rec[y].st = V.new_st;
+                sum += dg[k];
+            } else if (code[k] == 2) {
+                const uint32_t pos = s.warp_b[k * kWarps + warp] + (rnm[k] >> 16);
+                if (pos < kMeetCap) V.meet[pos] = make_uint2(xs[k], ys[k]);
+            }
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+    if (lane == 0 && sum) atomicAdd(&E->sum_new, sum);
+    __syncthreads();
+}
+
+// Takes tiles of entry e's level until none is left (owner and helpers).
+template <int BLOCK>
+__device__ void assist_work(SamplerSmem<BLOCK> &s, const SamplerLaunch &L, uint32_t e,
+                            bool owner) {
+    AssistEntry *E = L.assist.entries + e;
+    const uint32_t nt = s.lvl.ntiles;
+    for (;;) {
+        if (threadIdx.x == 0) {
+            const uint32_t t = atomicAdd(&E->claim, 1u);
+            if (t + 1u == nt) atomicAnd(&L.hdr->open_mask, ~(1u << e));  // the last tile is taken
+            s.a_tile = t;
+        }
+        __syncthreads();
+        const uint32_t t = s.a_tile;
+        if (t >= nt) break;
+        assist_tile<BLOCK>(s, L.assist, e, t);
+        if (threadIdx.x == 0) {
+            __threadfence();
+            atomicAdd(&E->done, 1u);
+            if (!owner) atomicAdd(&L.hdr->helper_tiles, 1u);
+        }
+    }
+    __syncthreads();
+}
+
+// The owner's side of a posted level (entry e, taken by acquire_entry):
+// the frontier's item prefix and tile table, its share of the tiles, the
+// results into the sample state, and the entry handed back.  Returns false,
+// with the entry freed and nothing changed, when the tile table would not
+// fit; the caller then runs expand_level.
+template <int BLOCK>
+__device__ bool expand_level_assisted(const SamplerLaunch &L, const SegDesc &A,
+                                      SamplerSmem<BLOCK> &s, NodeRec *rec, uint32_t *queue,
+                                      uint2 *meet, uint32_t side, uint32_t lo, uint32_t hi,
+                                      uint32_t depth, uint32_t e) {
+    constexpr int kTile = Shape<BLOCK>::kTile;
+    constexpr int kChunk = Shape<BLOCK>::kChunk;
+    constexpr int kPer = Shape<BLOCK>::kPerThread;
+    const AssistBoard &B = L.assist;
+    AssistEntry *E = B.entries + e;
+    const uint32_t *off = side == kSideU ? A.out_off : A.in_off;
+    const uint32_t *adj = side == kSideU ? A.out_adj : A.in_adj;
+    const uint32_t F = hi - lo;
+    const uint64_t tb = (uint64_t)e * B.tile_cap;
+    uint32_t *pre = B.pre + (uint64_t)e * (B.node_cap + 1u);
+    uint32_t *rs = B.rs + (uint64_t)e * B.node_cap;
+    uint4 *tiles = B.tiles + tb;
+    // item prefix, row starts, and the tiles, each starting in the node that
+    // holds its first item
+    uint32_t carry = 0, tcarry = 0;
+    for (uint32_t c0 = 0; c0 < F; c0 += kChunk) {
+        const uint32_t nc = min((uint32_t)kChunk, F - c0);
+        uint32_t xq[kPer], o0[kPer], o1[kPer];
+#pragma unroll
+        for (int i = 0; i < kPer; i++) {
+            const uint32_t p = threadIdx.x * kPer + i;
+            xq[i] = p < nc ? __ldcg(&queue[lo + c0 + p]) : 0u;
+        }
+        uint32_t tsum = 0;
+#pragma unroll
+        for (int i = 0; i < kPer; i++) {
+            const uint32_t p = threadIdx.x * kPer + i;
+            o0[i] = o1[i] = 0u;
+            if (p < nc) {
+                o0[i] = __ldg(&off[xq[i]]);
+                o1[i] = __ldg(&off[xq[i] + 1]);
+            }
+            tsum += o1[i] - o0[i];
+        }
+        uint32_t excl;
+        const uint32_t total = block_exclusive_scan<BLOCK>(tsum, excl, s.scan_tmp);
+#pragma unroll
+        for (int i = 0; i < kPer; i++) {
+            const uint32_t p = threadIdx.x * kPer + i;
+            const uint32_t d = o1[i] - o0[i];
+            if (p < nc) {
+                pre[c0 + p] = carry + excl;
+                rs[c0 + p] = o0[i];
+                for (uint64_t j = ((uint64_t)excl + kTile - 1) / kTile;
+                     j * kTile < (uint64_t)excl + d; j++) {
+                    const uint64_t ti = (uint64_t)tcarry + j;
+                    if (ti < B.tile_cap)
+                        tiles[ti] = make_uint4(c0 + p, 0u, carry + (uint32_t)(j * kTile),
+                                               carry + (uint32_t)min((j + 1) * kTile,
+                                                                     (uint64_t)total));
+                }
+            }
+            excl += d;
+        }
+        carry += total;
+        tcarry += (total + kTile - 1) / kTile;
+    }
+    if (threadIdx.x == 0) pre[F] = carry;
+    __syncthreads();
+    const bool fits = tcarry >= 1u && tcarry <= B.tile_cap;
+    if (fits) {
+        // nodes to stage per tile: up to the node of the next tile's first
+        // item in the same chunk, else to the chunk's end; look-back words
+        // cleared
+        for (uint32_t t = threadIdx.x; t < tcarry; t += BLOCK) {
+            const uint32_t l0 = __ldcg(reinterpret_cast<const uint32_t *>(&tiles[t]));
+            const uint32_t c = l0 / (uint32_t)kChunk;
+            const uint32_t cend = (uint32_t)min((uint64_t)(c + 1u) * kChunk, (uint64_t)F);
+            uint32_t endn = cend;
+            if (t + 1u < tcarry) {
+                const uint32_t nx = __ldcg(reinterpret_cast<const uint32_t *>(&tiles[t + 1u]));
+                if (nx / (uint32_t)kChunk == c) endn = min(nx + 1u, cend);
+            }
+            reinterpret_cast<uint32_t *>(&tiles[t])[1] = endn - l0;
+            B.hit_flag[tb + t] = 0u;
+            B.cnt_flag[tb + t] = 0ull;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (fits) {
+            AssistLevel &V = s.lvl;
+            V.ntiles = tcarry;
+            V.items = carry;
+            V.nodes = F;
+            V.lo = lo;
+            V.new_st = st_make(side, depth + 1u);
+            V.side = side;
+            V.qbase = s.end_q;
+            V.mbase = s.nmeet;
+            V.off = off;
+            V.adj = adj;
+            V.rec = rec;
+            V.queue = queue;
+            V.meet = meet;
+            E->lvl = V;
+            E->claim = 0u;
+            E->done = 0u;
+            E->ntiles = tcarry;
+            E->hits = 0u;
+            E->sum_new = 0u;
+            E->joins = 0u;
+            E->meets = 0u;
+            E->err = 0u;
+            __threadfence();
+            st_release_u32(&E->state, (s.a_state & ~3u) | 2u);
+            atomicOr(&L.hdr->open_mask, 1u << e);
+        } else {
+            st_release_u32(&E->state, ((s.a_state >> 2) + 1u) << 2);
+        }
+    }
+    __syncthreads();
+    if (!fits) return false;
+    assist_work<BLOCK>(s, L, e, true);
+    if (threadIdx.x == 0) {
+        const bool ok = wait_at_least(&E->done, tcarry);
+        __threadfence();
+        if (ok && __ldcg(&E->err) == 0u) {
+            const AssistLevel &V = s.lvl;
+            s.end_q = V.qbase + __ldcg(&E->joins);
+            const uint64_t mt = (uint64_t)V.mbase + __ldcg(&E->meets);
+            if (mt > kMeetCap && s.status == 0) s.status = SILVAN_E_CAPACITY;
+            s.nmeet = (uint32_t)min(mt, (uint64_t)kMeetCap);
+            s.vis += V.items;
+            s.sum_new = __ldcg(&E->sum_new);
+            s.pred_hits += __ldcg(&E->hits);
+            atomicAdd(&L.hdr->assisted, 1u);
+        } else {
+            s.status = SILVAN_E_TIMEOUT;
+            s.sum_new = 0u;
+        }
+        // hand the entry on only when no helper is inside any more: a helper
+        // either shows in `inside` here or sees the closed state and leaves
+        atomicAnd(&L.hdr->open_mask, ~(1u << e));
+        atomicExch(&E->state, (s.a_state & ~3u) | 3u);
+        __threadfence();
+        if (wait_zero(&E->inside)) st_release_u32(&E->state, ((s.a_state >> 2) + 1u) << 2);
+        else if (s.status == 0) s.status = SILVAN_E_TIMEOUT;  // the entry stays closed
+    }
+    return true;
+}
+
+// Helps the posted level thread 0 entered (s.a_entry), then leaves it.
+template <int BLOCK>
+__device__ void help_entry(const SamplerLaunch &L, SamplerSmem<BLOCK> &s, uint32_t e) {
+    assist_work<BLOCK>(s, L, e, false);
+    if (threadIdx.x == 0) {
+        __threadfence();
+        atomicSub(&L.assist.entries[e].inside, 1u);
+    }
+}
+
 template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK, Shape<BLOCK>::kMinBlocks) sampler_kernel(SamplerLaunch L) {
     constexpr int kWarps = Shape<BLOCK>::kWarps;
@@ -514,23 +1124,61 @@ __global__ void __launch_bounds__(BLOCK, Shape<BLOCK>::kMinBlocks) sampler_kerne
     const uint32_t nsegs = L.hdr->nsegs;
     const SegDesc &A = s.seg;
 
+    // Between two samples, a posted level that has tiles left comes first.
+    // Once the round has no sample left, the CTA keeps helping posted levels
+    // until every sample is done (or it has polled kAssistPolls times).  The
+    // loop's own state lives in shared memory, out of the registers of the
+    // sample code.
+    if (threadIdx.x == 0) {
+        s.a_drained = 0;
+        s.a_polls = 0;
+        s.a_nap = 256;
+    }
     for (;;) {
         if (threadIdx.x == 0) {
-            const uint32_t w = atomicAdd(&L.hdr->work, 1u);
-            s.work = w;
-            if (w < total) {
-                // segment owning work index w: last segment with base <= w
-                uint32_t l = 0, h = nsegs;
-                while (h - l > 1) {
-                    const uint32_t mid = (l + h) >> 1;
-                    if (L.segs[mid].base <= w) l = mid;
-                    else h = mid;
+            int32_t pick = L.assist.entries != nullptr ? join_entry<BLOCK>(L, s, blockIdx.x) : -1;
+            if (pick < 0 && !s.a_drained) {
+                const uint32_t w = atomicAdd(&L.hdr->work, 1u);
+                s.work = w;
+                if (w < total) {
+                    // segment owning work index w: last segment with base <= w
+                    uint32_t l = 0, h = nsegs;
+                    while (h - l > 1) {
+                        const uint32_t mid = (l + h) >> 1;
+                        if (L.segs[mid].base <= w) l = mid;
+                        else h = mid;
+                    }
+                    s.sample = l;
+                    pick = -3;  // a sample
                 }
-                s.sample = l;
             }
+            if (pick == -1) {
+                // no sample left: wait for posted levels, or leave
+                s.a_drained = 1;
+                if (L.assist.entries == nullptr || ++s.a_polls > kAssistPolls ||
+                    ld_acquire_u32(&L.hdr->finished) >= total) {
+                    pick = -2;
+                } else {
+                    __nanosleep(s.a_nap);
+                    s.a_nap = min(s.a_nap * 2u, 16384u);
+                }
+            } else {
+                s.a_nap = 256;
+            }
+            s.a_entry = pick;
         }
         __syncthreads();
-        if (s.work >= total) break;
+        const int32_t pick = s.a_entry;
+        if (pick >= 0) {
+            help_entry<BLOCK>(L, s, (uint32_t)pick);
+            __syncthreads();
+            continue;
+        }
+        if (pick == -2) break;
+        if (pick == -1) {
+            __syncthreads();
+            continue;
+        }
         {
             const uint32_t *src = reinterpret_cast<const uint32_t *>(&L.segs[s.sample]);
             uint32_t *dst = reinterpret_cast<uint32_t *>(&s.seg);
@@ -572,6 +1220,7 @@ __global__ void __launch_bounds__(BLOCK, Shape<BLOCK>::kMinBlocks) sampler_kerne
                 const unsigned long long dc = (unsigned long long)(clock64() - t_sample0);
                 atomicAdd(&L.hdr->cycles, dc);
                 atomicMax(&L.hdr->max_cycles, dc);
+                atomicAdd(&L.hdr->finished, 1u);
             }
             __syncthreads();
             continue;
@@ -608,8 +1257,15 @@ __global__ void __launch_bounds__(BLOCK, Shape<BLOCK>::kMinBlocks) sampler_kerne
             const uint32_t hi = side_u ? s.end_u : s.end_v;
             const uint32_t depth = side_u ? s.depth_u : s.depth_v;
             const uint32_t q0 = s.end_q;
+            if (threadIdx.x == 0)
+                s.a_entry = (L.assist.entries != nullptr && A.assist_items != 0u)
+                                ? post_level<BLOCK>(L, s, side_u, lo, hi, depth)
+                                : -1;
             __syncthreads();
-            expand_level(A, s, rec, queue, meet, exp_side, lo, hi, depth);
+            if (s.a_entry < 0 ||
+                !expand_level_assisted<BLOCK>(L, A, s, rec, queue, meet, exp_side, lo, hi, depth,
+                                              (uint32_t)s.a_entry))
+                expand_level(A, s, rec, queue, meet, exp_side, lo, hi, depth);
             if (threadIdx.x == 0) {
                 if (depth + 1 < (uint32_t)kMaxLevels) {
                     s.lvl_lo[side_u ? 0 : 1][depth + 1] = q0;
@@ -839,6 +1495,8 @@ __global__ void __launch_bounds__(BLOCK, Shape<BLOCK>::kMinBlocks) sampler_kerne
             const unsigned long long dc = (unsigned long long)(clock64() - t_sample0);
             atomicAdd(&L.hdr->cycles, dc);
             atomicMax(&L.hdr->max_cycles, dc);
+            __threadfence();
+            atomicAdd(&L.hdr->finished, 1u);
         }
         __syncthreads();
     }
@@ -849,6 +1507,10 @@ __global__ void round_begin_kernel(SamplerLaunch L, uint32_t max_segs) {
     for (uint32_t i = threadIdx.x; i < ns; i += blockDim.x) *L.segs[i].rec_cursor = 0ull;
     if (threadIdx.x == 0) {
         L.hdr->work = 0;
+        L.hdr->finished = 0;
+        L.hdr->open_mask = 0;
+        L.hdr->assisted = 0;
+        L.hdr->helper_tiles = 0;
         L.hdr->cycles = 0;
         L.hdr->max_cycles = 0;
     }
@@ -868,6 +1530,38 @@ cudaError_t sampler_init_slots(NodeRec *rec, uint32_t *hits, uint64_t total_node
                                cudaStream_t stream) {
     init_slots_kernel<<<1184, 256, 0, stream>>>(rec, hits, total_nodes);
     return cudaGetLastError();
+}
+
+namespace {
+constexpr uint32_t kAssistTileCap = 1u << 16;
+uint64_t align256(uint64_t b) { return (b + 255u) & ~255ull; }
+}  // namespace
+
+uint64_t assist_board_bytes(uint64_t n) {
+    return align256(sizeof(AssistEntry) * kAssistEntries) +
+           align256(4ull * (n + 1) * kAssistEntries) + align256(4ull * n * kAssistEntries) +
+           align256(16ull * kAssistTileCap * kAssistEntries) +
+           align256(4ull * kAssistTileCap * kAssistEntries) +
+           align256(8ull * kAssistTileCap * kAssistEntries);
+}
+
+cudaError_t assist_board_init(AssistBoard *b, void *mem, uint64_t n, cudaStream_t stream) {
+    if (n >= 0x7fffffffull) return cudaErrorInvalidValue;  // joins fit the look-back words
+    char *p = static_cast<char *>(mem);
+    b->entries = reinterpret_cast<AssistEntry *>(p);
+    p += align256(sizeof(AssistEntry) * kAssistEntries);
+    b->pre = reinterpret_cast<uint32_t *>(p);
+    p += align256(4ull * (n + 1) * kAssistEntries);
+    b->rs = reinterpret_cast<uint32_t *>(p);
+    p += align256(4ull * n * kAssistEntries);
+    b->tiles = reinterpret_cast<uint4 *>(p);
+    p += align256(16ull * kAssistTileCap * kAssistEntries);
+    b->hit_flag = reinterpret_cast<uint32_t *>(p);
+    p += align256(4ull * kAssistTileCap * kAssistEntries);
+    b->cnt_flag = reinterpret_cast<unsigned long long *>(p);
+    b->node_cap = (uint32_t)n;
+    b->tile_cap = kAssistTileCap;
+    return cudaMemsetAsync(b->entries, 0, sizeof(AssistEntry) * kAssistEntries, stream);
 }
 
 cudaError_t sampler_round_begin(const SamplerLaunch &L, uint32_t max_segs, cudaStream_t stream) {

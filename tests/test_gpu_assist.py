@@ -1,0 +1,94 @@
+"""Wide BFS levels expanded by several CTAs (the sampler's help board): a
+level posted after a round's last sample was taken is expanded in three
+sweeps over tiles by its owner and the idle CTAs.  The level's queue order,
+predecessor keys, counts, sigma and meeting list must be exactly those of the
+one-CTA expansion (silvan/src/Sp_sampler.cpp:116-143), so whole runs must
+leave the oracle's counters bit for bit; a threshold of one item posts every
+level of the last samples, which exercises entries taken, opened, joined and
+handed on many times per launch."""
+import numpy as np
+import pytest
+
+from conftest import port_graph
+
+pytestmark = pytest.mark.gpu
+
+SCALARS = ["num_samples", "vis_edges", "iteration_index", "num_partitions", "omega",
+           "first_stopping_samples", "last_stopping_samples", "alpha_sp_sampling",
+           "union_sample", "first_pass_samples", "stop_reason", "void_samples",
+           "backtracked_paths", "ball_nodes", "pred_entries"]
+NEVER = 0xFFFFFFFF
+
+
+def same_counters(ja, jb):
+    a, b = ja.counters(), jb.counters()
+    for f in ("approx", "wimpy", "mcrade", "partition_index"):
+        np.testing.assert_array_equal(a[f], b[f], err_msg=f)
+
+
+@pytest.mark.parametrize("name,block,form,items,extra", [
+    ("rmat11d", 128, "batched", 1, {}),
+    ("rmat11d", 1024, "batched", 1, {}),
+    ("rmat11d", 512, "plain", 1, {}),
+    ("rmat11u", 256, "batched", 64, {"alpha": 3.0, "alpha_given": True}),
+    ("ba2k", 512, "batched", 1, {}),
+    ("grid40", 128, "batched", 1, {"alpha": 0.0, "alpha_given": True}),
+    ("er3k", 1024, "plain", 16, {"k": 8}),
+])
+def test_assisted_levels_match_oracle(sb, port, small_graphs, name, block, form, items, extra):
+    hg, csr, _ = small_graphs[name]
+    eps = 0.08 if extra.get("k") else 0.03
+    job = sb.Probabilistic(sb.Graph.from_host(hg), eps, 0.1, seed=5, block=block, form=form,
+                           assist_items=items, **extra)
+    res = job.run()
+    assert res["assisted_levels"] > 0
+    o = port_graph(port, csr).run(csr.diameter, eps, 0.1, seed=5, **extra)
+    for f in ("num_samples", "vis_edges", "iteration_index", "num_partitions", "omega",
+              "first_stopping_samples", "last_stopping_samples", "alpha_sp_sampling",
+              "union_sample", "first_pass_samples", "stop_reason"):
+        assert res[f] == o[f], (f, res[f], o[f])
+    c = job.counters()
+    np.testing.assert_array_equal(c["approx"], o["approx"])
+    np.testing.assert_array_equal(c["wimpy"], o["wimpy"])
+    np.testing.assert_array_equal(c["mcrade"], o["mcrade"])
+    if extra.get("k"):
+        nodes, _ = job.topk()
+        np.testing.assert_array_equal(nodes, o["ranking_elements"][:len(nodes)])
+
+
+@pytest.mark.parametrize("scale,directed,items", [(15, True, 1), (16, True, 2048),
+                                                  (15, False, 512)])
+def test_assisted_and_alone_give_the_same_run(sb, scale, directed, items):
+    """Larger R-MAT graphs, whose hub levels reach thousands of entries: the
+    run with the help board and the run with every level on its own CTA
+    agree in every counter and result field."""
+    hg = sb.HostGraph.from_pairs(sb.rmat(scale, 16, scale, directed), directed)
+    g = sb.Graph.from_host(hg)
+    runs = []
+    for ai in (items, NEVER):
+        job = sb.Probabilistic(g, 0.01, 0.1, seed=3, assist_items=ai)
+        res = job.run()
+        runs.append((job, res))
+    (ja, ra), (jb, rb) = runs
+    assert ra["assisted_levels"] > 0 and ra["helper_tiles"] > 0
+    assert rb["assisted_levels"] == 0 and rb["helper_tiles"] == 0
+    for f in SCALARS:
+        assert ra[f] == rb[f], (f, ra[f], rb[f])
+    same_counters(ja, jb)
+
+
+def test_replay_with_assisted_levels_matches_oracle(sb, port):
+    """Per-sample records (path, path count, visited edges) of the replay hook
+    while the help board is in use (the default threshold, on a graph whose
+    hub levels pass it), against the oracle sample by sample."""
+    hg = sb.HostGraph.from_pairs(sb.rmat(15, 16, 7, True), True)
+    csr = hg.csr()
+    g = sb.Graph.from_host(hg)
+    got = g.replay(11, 0, 4000, 2.3)
+    assert (got["status"] == 0).all()
+    want = port_graph(port, csr).replay(11, 0, 4000, 2.3)
+    for f in ("path_length", "num_paths", "vis_edges"):
+        np.testing.assert_array_equal(got[f], getattr(want, f), err_msg=f)
+    np.testing.assert_array_equal(got["offsets"], want.offsets)
+    np.testing.assert_array_equal(got["nodes"], want.nodes)
+    np.testing.assert_array_equal(got["counts"], want.counts)
