@@ -10,7 +10,9 @@
 // short-option set is unchanged): --plain (one launch sequence per 11-sample
 // block), --seed N (job seed), --np-cap N (paths per sample), --slots N,
 // --block N (threads per sampler slot; default autotuned), --sigma-weighted
-// (the path-count-weighted backtrack instead of the reference's rule).
+// (the path-count-weighted backtrack instead of the reference's rule),
+// --assist-items N (BFS levels of at least N adjacency entries are expanded
+// by several sampler CTAs; 0 = default, 4294967295 = never).
 #include <cerrno>
 #include <climits>
 #include <cstdio>
@@ -40,7 +42,7 @@ double peeling_a = 2.0;
 bool m_hat = true;
 bool plain = false;
 uint64_t seed = 42;
-uint32_t np_cap = 0, slots = 0, block = 0;
+uint32_t np_cap = 0, slots = 0, block = 0, assist_items = 0;
 bool sigma_weighted = false;
 
 // silvan/main.cpp:51-68
@@ -72,6 +74,9 @@ void usage(const char *b) {
               << std::endl;
     std::cerr << "\t--sigma-weighted: pick predecessors by path count (not the reference's rule)"
               << std::endl;
+    std::cerr << "\t--assist-items N: levels of at least N entries on several CTAs "
+                 "(0 default, 4294967295 never)"
+              << std::endl;
 }
 
 // silvan/main.cpp:74-153: 0 ok, 1 error, 2 help
@@ -82,6 +87,7 @@ int parse(int argc, char **argv) {
                                        {"slots", required_argument, nullptr, 4},
                                        {"block", required_argument, nullptr, 5},
                                        {"sigma-weighted", no_argument, nullptr, 6},
+                                       {"assist-items", required_argument, nullptr, 7},
                                        {nullptr, 0, nullptr, 0}};
     int opt;
     while ((opt = getopt_long(argc, argv, "dhmk:o:s:a:v:", longopts, nullptr)) != -1) {
@@ -128,6 +134,7 @@ int parse(int argc, char **argv) {
             case 4: slots = (uint32_t)std::strtoul(optarg, nullptr, 10); break;
             case 5: block = (uint32_t)std::strtoul(optarg, nullptr, 10); break;
             case 6: sigma_weighted = true; break;
+            case 7: assist_items = (uint32_t)std::strtoul(optarg, nullptr, 10); break;
             default: break;
         }
     }
@@ -198,6 +205,7 @@ int main(int argc, char **argv) {
     p.np_cap = np_cap;
     p.slots = slots;
     p.block = block;
+    p.assist_items = assist_items;
     p.backtrack = sigma_weighted ? SILVAN_BACKTRACK_SIGMA_WEIGHTED : SILVAN_BACKTRACK_REFERENCE;
     silvan_job_t j = nullptr;
     rc = silvan_job_create(g, &p, &j);

@@ -97,3 +97,22 @@ def test_cli_output_and_file(sb, port, small_graphs, tmp_path, name, flags):
         assert row[2] == ref_row[2]
         if k == 0:
             assert row[3] == ref_row[3]  # tau-sized first pass
+
+
+def test_cli_assist_items_gives_the_same_output(sb, small_graphs, tmp_path):
+    """--assist-items only changes how wide levels are expanded (by several
+    sampler CTAs), never the estimates: the -o files and the sample counts
+    of a run that posts every level, one that posts none and the default
+    agree."""
+    hg, csr, directed = small_graphs["rmat11d"]
+    gpath = str(tmp_path / "g.txt")
+    write_graph(gpath, csr)
+    outs = []
+    for items in (None, "1", "4294967295"):
+        out = str(tmp_path / f"out_{items}.txt")
+        extra = [] if items is None else ["--assist-items", items]
+        r = run_bin(sb.CLI_PATH, ["-d", "--seed", "3", *extra, "-o", out, "0.03", "0.1", gpath])
+        assert r.returncode == 0, r.stderr
+        row = scrape(r.stdout)
+        outs.append((row[0], row[3], open(out).read()))
+    assert outs[0] == outs[1] == outs[2]
