@@ -755,6 +755,10 @@ def main():
                        "l2": "working set above L2 (CSR + per-slot state)",
                        "sampler_block": [r["sampler_block"] for r in results],
                        "sampler_launches_per_step": sum(r["sampler_launches"] for r in results)
+                       / args.steps,
+                       "wide_levels_shared_per_step": sum(r["assisted_levels"] for r in results)
+                       / args.steps,
+                       "helper_tiles_per_step": sum(r["helper_tiles"] for r in results)
                        / args.steps},
             "time_to_guarantee_ms": 1000 * t_max / args.steps,
             "samples_per_step": samples_all / max(1, world) / args.steps,

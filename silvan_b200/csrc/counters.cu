@@ -27,18 +27,15 @@ __device__ __forceinline__ uint32_t round_records(const RoundBuffers &rb, const 
     return (uint32_t)min((uint64_t)a.n_records, rb.rec_cap);
 }
 
-__global__ void signs_kernel(const ApplyState *st) {
-    const RoundBuffers rb = st->rb;
-    const ApplyArgs a = st->a;
-    if (a.pass != 2) return;
-    for (uint32_t s = a.lo + blockIdx.x * blockDim.x + threadIdx.x; s < a.hi;
-         s += gridDim.x * blockDim.x)
-        rb.signs[s] = rademacher_mask(a.seed, a.first_sample + s);
-}
-
+// The Rademacher signs of the round's samples (pass 2), and the records per
+// node with the list of touched nodes.
 __global__ void bucket_count_kernel(const ApplyState *st) {
     const RoundBuffers rb = st->rb;
     const ApplyArgs a = st->a;
+    if (a.pass == 2)
+        for (uint32_t s = a.lo + blockIdx.x * blockDim.x + threadIdx.x; s < a.hi;
+             s += gridDim.x * blockDim.x)
+            rb.signs[s] = rademacher_mask(a.seed, a.first_sample + s);
     const uint32_t R = round_records(rb, a);
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < R; i += gridDim.x * blockDim.x) {
         PathRec r = rb.recs[i];
@@ -85,17 +82,24 @@ __global__ void scan_reduce_kernel(const ApplyState *st) {
     if (threadIdx.x == 0) rb.block_sums[blockIdx.x] = s;
 }
 
+// One warp: exclusive scan of the block sums, 32 at a time.
 __global__ void scan_top_kernel(const ApplyState *st, int nblocks) {
     const RoundBuffers rb = st->rb;
-    if (threadIdx.x == 0 && blockIdx.x == 0) {
-        uint32_t acc = 0;
-        for (int i = 0; i < nblocks; i++) {
-            uint32_t t = rb.block_sums[i];
-            rb.block_sums[i] = acc;
-            acc += t;
+    const int lane = threadIdx.x & 31;
+    if (blockIdx.x != 0 || threadIdx.x >= 32) return;
+    uint32_t acc = 0;
+    for (int i0 = 0; i0 < nblocks; i0 += 32) {
+        const int i = i0 + lane;
+        const uint32_t v = i < nblocks ? rb.block_sums[i] : 0u;
+        uint32_t incl = v;
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += t;
         }
-        rb.block_sums[nblocks] = acc;
+        if (i < nblocks) rb.block_sums[i] = acc + incl - v;
+        acc += __shfl_sync(0xffffffffu, incl, 31);
     }
+    if (lane == 0) rb.block_sums[nblocks] = acc;
 }
 
 __global__ void scan_down_kernel(const ApplyState *st) {
@@ -333,7 +337,7 @@ __global__ void __launch_bounds__(1024) apply_large_kernel(const ApplyState *st)
     }
 }
 
-__global__ void commit_kernel(const ApplyState *st) {
+__device__ void commit_sums(const ApplyState *st) {
     const RoundBuffers rb = st->rb;
     const JobCounters jc = st->jc;
     const ApplyArgs a = st->a;
@@ -373,7 +377,10 @@ __global__ void commit_kernel(const ApplyState *st) {
     }
 }
 
-__global__ void reset_touched_kernel(const ApplyState *st) {
+// The round's scalar sums (commit_sums) and the per-node cursors zeroed for
+// the next round; neither depends on the folds.
+__global__ void commit_kernel(const ApplyState *st) {
+    commit_sums(st);
     const RoundBuffers rb = st->rb;
     const uint32_t T = *rb.n_touched;
     for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < T; t += gridDim.x * blockDim.x)
@@ -504,7 +511,6 @@ cudaError_t apply_init() {
 
 cudaError_t apply_round(const ApplyState *st, uint32_t *n_touched, cudaStream_t stream) {
     cudaMemsetAsync(n_touched, 0, 2 * sizeof(uint32_t), stream);  // n_touched, n_large
-    signs_kernel<<<64, 256, 0, stream>>>(st);
     bucket_count_kernel<<<592, 256, 0, stream>>>(st);
     scan_reduce_kernel<<<kScanBlocks, kScanThreads, 0, stream>>>(st);
     scan_top_kernel<<<1, 32, 0, stream>>>(st, kScanBlocks);
@@ -512,8 +518,7 @@ cudaError_t apply_round(const ApplyState *st, uint32_t *n_touched, cudaStream_t 
     bucket_scatter_kernel<<<592, 256, 0, stream>>>(st);
     apply_small_kernel<<<592, kApplyThreads, 0, stream>>>(st);
     apply_large_kernel<<<148, 1024, kLargeBucket * sizeof(unsigned long long), stream>>>(st);
-    commit_kernel<<<16, 256, 0, stream>>>(st);
-    reset_touched_kernel<<<148, 256, 0, stream>>>(st);
+    commit_kernel<<<148, 256, 0, stream>>>(st);
     return cudaGetLastError();
 }
 
