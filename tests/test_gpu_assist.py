@@ -1,10 +1,11 @@
 """Wide BFS levels expanded by several CTAs (the sampler's help board): a
-level posted after a round's last sample was taken is expanded in three
-sweeps over tiles by its owner and the idle CTAs.  The level's queue order,
-predecessor keys, counts, sigma and meeting list must be exactly those of the
-one-CTA expansion (silvan/src/Sp_sampler.cpp:116-143), so whole runs must
-leave the oracle's counters bit for bit; a threshold of one item posts every
-level of the last samples, which exercises entries taken, opened, joined and
+posted level is expanded tile by tile by its owner and by the CTAs that are
+between samples or out of samples, with look-backs over the tiles in place
+of the one-CTA tile order.  The level's queue order, predecessor keys,
+counts, sigma and meeting list must be exactly those of the one-CTA
+expansion (silvan/src/Sp_sampler.cpp:116-143), so whole runs must leave the
+oracle's counters bit for bit; a threshold of one item posts every level
+whenever an entry is free, which exercises entries taken, opened, joined and
 handed on many times per launch."""
 import numpy as np
 import pytest
