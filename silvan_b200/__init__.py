@@ -369,7 +369,16 @@ class Graph:
 class Probabilistic:
     """Mirror of the reference's estimator object (silvan/include/
     Probabilistic.h:27-56): construct with the graph and the binary's flags,
-    call run(), read the centralities."""
+    call run(), read the centralities.
+
+    Beyond the binary's flags: `seed` (the Philox key of the sample stream),
+    `form` ("batched" or "plain"), `np_cap` (paths per sample), `slots` and
+    `block` (sampler slots and threads per slot; 0 = chosen by the engine),
+    `threads` (the divisor of union_sample; 1 = parity mode), `backtrack`
+    ("reference", or "sigma" for path-count-weighted predecessors) and
+    `assist_items` (BFS levels of at least this many adjacency entries are
+    expanded by several sampler CTAs; 0 = 32 x the CTA size, 0xFFFFFFFF =
+    never).  Only `seed` and `backtrack` change the estimates."""
 
     def __init__(self, graph: Graph, eps, delta, k=0, alpha=2.3, alpha_given=False, a=2.0,
                  m_hat=True, seed=42, form="batched", verbose=0.0, np_cap=0, slots=0,
