@@ -378,7 +378,8 @@ class Probabilistic:
     ("reference", or "sigma" for path-count-weighted predecessors) and
     `assist_items` (BFS levels of at least this many adjacency entries are
     expanded by several sampler CTAs; 0 = 32 x the CTA size, 0xFFFFFFFF =
-    never).  Only `seed` and `backtrack` change the estimates."""
+    never).  Only `seed`, `backtrack` and, in top-k mode, `threads` change
+    the results."""
 
     def __init__(self, graph: Graph, eps, delta, k=0, alpha=2.3, alpha_given=False, a=2.0,
                  m_hat=True, seed=42, form="batched", verbose=0.0, np_cap=0, slots=0,
