@@ -93,20 +93,35 @@ def make_graph(cfg):
     return sb.HostGraph.from_pairs(pairs, cfg["directed"])
 
 
-def multigraph_hosts():
-    """The 64 graphs of the multi-graph workload."""
+def multigraph_sizes():
+    """(node count, seed) of the 64 graphs of the multi-graph workload: even
+    indices ER with mean degree 8, odd ones BA with 4 edges per node."""
     import math
 
     import numpy as np
-    import silvan_b200 as sb
     out = []
     for i in range(64):
         seed = 100 + i
         rng = np.random.default_rng(seed)
-        n = int(round(math.exp(rng.uniform(math.log(1e3), math.log(2e6)))))
+        out.append((int(round(math.exp(rng.uniform(math.log(1e3), math.log(2e6))))), seed))
+    return out
+
+
+def multigraph_hosts():
+    """The 64 graphs of the multi-graph workload."""
+    import silvan_b200 as sb
+    out = []
+    for i, (n, seed) in enumerate(multigraph_sizes()):
         pairs = sb.erdos_renyi(n, 8.0, seed) if i % 2 == 0 else sb.barabasi_albert(n, 4, seed)
         out.append(sb.HostGraph.from_pairs(pairs, False))
     return out
+
+
+def multigraph_ref_csrs(lib):
+    """The same 64 graphs through the reference harness's generators."""
+    return [RefCSR(lib, 1, n, 0, 0, 8.0, 0, seed, False) if i % 2 == 0 else
+            RefCSR(lib, 0, n, 4, 0, 0, 0, seed, False)
+            for i, (n, seed) in enumerate(multigraph_sizes())]
 
 
 def job_kwargs(cfg):
@@ -176,6 +191,12 @@ def refbench_lib():
     if not os.path.exists(path):
         return None
     lib = C.CDLL(path)
+    lib.refbench_graph_new.restype = C.c_void_p
+    lib.refbench_graph_new.argtypes = [C.c_int, C.c_uint32, C.c_uint32, C.c_uint32, C.c_double,
+                                       C.c_double, C.c_uint64, C.c_int]
+    lib.refbench_graph_info.argtypes = [C.c_void_p] * 4
+    lib.refbench_graph_csr.argtypes = [C.c_void_p] * 5
+    lib.refbench_graph_free.argtypes = [C.c_void_p]
     lib.refbench_run.restype = C.c_int
     lib.refbench_run.argtypes = [C.c_uint32, C.c_int] + [C.c_void_p] * 4 + \
         [C.c_double, C.c_double, C.c_uint32, C.c_double, C.c_int, C.c_double, C.c_int, C.c_int] + \
@@ -184,6 +205,56 @@ def refbench_lib():
     lib.refbench_sample.argtypes = [C.c_uint32, C.c_int] + [C.c_void_p] * 4 + \
         [C.c_double, C.c_int, C.c_uint64, C.c_void_p, C.c_void_p, C.c_void_p]
     return lib
+
+
+class RefCSR:
+    """A benchmark graph built by the reference harness (no product library):
+    the fields reference_run and reference_sample read."""
+
+    def __init__(self, lib, kind, a, b, c, x, y, seed, directed):
+        import numpy as np
+        h = lib.refbench_graph_new(kind, a, b, c, x, y, seed, int(directed))
+        if not h:
+            raise RuntimeError("reference harness could not generate the graph")
+        n, mo, mi = C.c_uint32(), C.c_uint64(), C.c_uint64()
+        lib.refbench_graph_info(h, C.byref(n), C.byref(mo), C.byref(mi))
+        self.n, self.directed = n.value, bool(directed)
+        self.out_off = np.zeros(self.n + 1, np.uint64)
+        self.out_adj = np.zeros(max(1, mo.value), np.uint32)
+        self.in_off = np.zeros(self.n + 1, np.uint64) if directed else self.out_off
+        self.in_adj = np.zeros(max(1, mi.value), np.uint32) if directed else self.out_adj
+        lib.refbench_graph_csr(h, self.out_off.ctypes.data, self.out_adj.ctypes.data,
+                               self.in_off.ctypes.data, self.in_adj.ctypes.data)
+        lib.refbench_graph_free(h)
+        self.out_adj = self.out_adj[:mo.value]
+        self.in_adj = self.in_adj[:mi.value] if directed else self.out_adj
+
+
+def ref_graph(lib, cfg):
+    """The workload's graph through the reference harness's copy of the
+    generators (the same seeded graphs as make_graph)."""
+    if cfg["gen"] == "rmat":
+        return RefCSR(lib, 2, cfg["scale"], cfg["edge_factor"], int(cfg["directed"]), 0, 0,
+                      cfg["seed"], cfg["directed"])
+    if cfg["gen"] == "grid":
+        return RefCSR(lib, 3, cfg["side"], 0, 0, cfg["delete"], cfg["shortcut"], cfg["seed"],
+                      False)
+    return RefCSR(lib, 0, cfg["n"], cfg["m"], 0, 0, 0, cfg["seed"], cfg["directed"])
+
+
+def csr_checksum(csr):
+    """SHA-1 of the CSR rows (offsets as u64, then neighbours as u32; the
+    in-rows too for directed graphs): both arms print it for their graph."""
+    import hashlib
+
+    import numpy as np
+    h = hashlib.sha1()
+    h.update(np.ascontiguousarray(csr.out_off, np.uint64).tobytes())
+    h.update(np.ascontiguousarray(csr.out_adj, np.uint32).tobytes())
+    if csr.directed:
+        h.update(np.ascontiguousarray(csr.in_off, np.uint64).tobytes())
+        h.update(np.ascontiguousarray(csr.in_adj, np.uint32).tobytes())
+    return h.hexdigest()[:16]
 
 
 def reference_run(lib, csr, cfg, threads):
@@ -225,6 +296,21 @@ def cpu_reference(lib, csr, cfg, threads):
         what = ("one complete estimation of the benchmark graph by the reference's OpenMP "
                 "build ('Total time' window)")
     return r, what
+
+
+def cpu_reference_stats(lib, csr, cfg, threads, runs=3, warmup=1):
+    """cpu_reference after `warmup` untimed runs, `runs` times: the median
+    rate and the spread, so that the CPU leg of the GPU arm and the
+    reference arm measure the same thing the same way."""
+    for _ in range(warmup):
+        cpu_reference(lib, csr, cfg, threads)
+    rates, what = [], ""
+    for _ in range(runs):
+        r, what = cpu_reference(lib, csr, cfg, threads)
+        rates.append(r["samples"] / r["total_time"])
+    return {"value": statistics.median(rates), "unit": "paths/s", "cores": threads,
+            "kind": "reference", "runs": runs, "min": min(rates), "max": max(rates),
+            "sample": f"median of {runs} x ({what}) after {warmup} untimed"}
 
 
 def combine_replicas(pg, samples, t_dev, e2e_samples, e2e_t, device="cpu"):
@@ -271,13 +357,15 @@ def run_reference_arm(args, cfg):
     threads = os.cpu_count() or 1
     holder = {}
     if cfg["kind"] == "multi":
-        csrs = [h.csr() for h in multigraph_hosts()[:8]]
-        holder["what"] = "complete estimations of the first 8 of the 64 graphs, one by one"
+        csrs = multigraph_ref_csrs(lib)
+        holder["what"] = "complete estimations of all 64 graphs, one by one"
+        checksum = None
 
         def run():
             return [reference_run(lib, c, cfg, threads) for c in csrs]
     else:
-        csr = make_graph(cfg).csr()
+        csr = ref_graph(lib, cfg)
+        checksum = csr_checksum(csr)
 
         def run():
             r, holder["what"] = cpu_reference(lib, csr, cfg, threads)
@@ -295,7 +383,8 @@ def run_reference_arm(args, cfg):
         "ms_per_step": 1000 * t / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u32/u64/f64", "data": "synthetic",
         "config": dict({"workload": cfg["workload"], "eps": cfg.get("eps"), "delta": cfg["delta"],
-                        "form": "reference OpenMP build", "parallelism": "host threads"},
+                        "form": "reference OpenMP build", "parallelism": "host threads",
+                        "csr_sha1_16": checksum},
                        **({} if cfg["kind"] == "multi" else job_kwargs(cfg))),
         "time_to_guarantee_ms": 1000 * t / args.steps,
         "cpu_baseline": {"value": val, "unit": "paths/s", "cores": threads, "kind": "reference",
@@ -416,11 +505,12 @@ def run_multi(args, cfg):
         lib = refbench_lib()
         if lib is not None:
             threads = os.cpu_count() or 1
-            rr = [reference_run(lib, c, cfg, threads) for c in csrs[:8]]
+            rr = [reference_run(lib, c, cfg, threads) for c in csrs]
             cpu = {"value": sum(r["samples"] for r in rr) / sum(r["total_time"] for r in rr),
                    "unit": "paths/s", "cores": threads, "kind": "reference",
-                   "sample": "complete estimations of the first 8 of the 64 graphs by the "
-                             "reference's OpenMP build, one after another"}
+                   "seconds": sum(r["total_time"] for r in rr),
+                   "sample": "complete estimations of all 64 graphs by the reference's "
+                             "OpenMP build, one after another ('Total time' windows summed)"}
     alg = sum(8 * r["vis_edges"] + 24 * r["ball_nodes"] + 4 * r["pred_entries"] for r in results)
     print(json.dumps({
         "metric": "paths/sec", "value": samples / t, "unit": "paths/s", "n_gpus": 1,
@@ -633,6 +723,9 @@ def main():
                          "memory for profiler captures")
     ap.add_argument("--block", type=int, default=0, choices=[0, 128, 256, 512, 1024],
                     help="threads per sampler slot (0 = autotuned per graph and round)")
+    ap.add_argument("--plain-steps", type=int, default=3,
+                    help="plain-form estimations on the first timed steps' seeds, for the "
+                         "batched-over-plain ratio (0 = skip)")
     ap.add_argument("--requests", type=int, default=200, help="serve: requests in the stream")
     ap.add_argument("--rate", type=float, default=4.0, help="serve: Poisson arrivals per second")
     ap.add_argument("--slo-ms", type=float, default=2500.0,
@@ -690,6 +783,28 @@ def main():
     t_dev = sum(r["time_device_s"] for r in results)
     launches = sum(r["kernel_launches"] for r in results)
 
+    # The plain form (one launch sequence per 11-sample block, as the
+    # reference's loop of Probabilistic.cpp:1054-1102 draws them) on the
+    # first timed steps' seeds, after the timed region: the batched form's
+    # speed-up on identical estimations.
+    plain = None
+    if args.form == "batched" and args.plain_steps > 0:
+        bt, pt, same = 0.0, 0.0, True
+        for s in range(min(args.plain_steps, args.steps)):
+            job = sb.Probabilistic(g, cfg["eps"], cfg["delta"], seed=seed0 + args.warmup + s,
+                                   form="plain", slots=args.slots, **job_kwargs(cfg))
+            r = job.run()
+            del job
+            pt += r["time_device_s"]
+            bt += results[s]["time_device_s"]
+            same = same and r["num_samples"] == results[s]["num_samples"] and \
+                r["vis_edges"] == results[s]["vis_edges"]
+        k = min(args.plain_steps, args.steps)
+        plain = {"plain_ms_per_estimation": 1000 * pt / k,
+                 "batched_ms_per_estimation": 1000 * bt / k,
+                 "batched_over_plain": pt / bt if bt > 0 else None, "estimations": k,
+                 "same_results": same}
+
     # e2e through the C-ABI from pinned host buffers: CSR upload, job
     # creation, the run and the read-back of every estimate, per step
     keep = []
@@ -738,10 +853,7 @@ def main():
         if not args.no_cpu_baseline:
             lib = refbench_lib()
             if lib is not None:
-                threads = os.cpu_count() or 1
-                rr, what = cpu_reference(lib, csr, cfg, threads)
-                cpu = {"value": rr["samples"] / rr["total_time"], "unit": "paths/s",
-                       "cores": threads, "kind": "reference", "sample": what}
+                cpu = cpu_reference_stats(lib, csr, cfg, os.cpu_count() or 1)
         line = {
             "metric": "paths/sec", "value": samples_all / t_max, "unit": "paths/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -749,6 +861,7 @@ def main():
             "scaling": "weak", "vs_baseline": None, "dtype": "u32/u64/f64",
             "data": "synthetic",
             "config": {"workload": cfg["workload"], "n": csr.n, "m": int(csr.out_off[-1]),
+                       "csr_sha1_16": csr_checksum(csr),
                        "eps": cfg["eps"], "delta": cfg["delta"], "form": args.form,
                        **job_kwargs(cfg),
                        "parallelism": "replicas" if world > 1 else "single",
@@ -784,6 +897,8 @@ def main():
             "gpu_launches": launches,
             "clocks": clk.summary(),
         }
+        if plain is not None:
+            line["plain_vs_batched"] = plain
         if cfg.get("alpha_given") and cfg.get("gen") == "grid":
             line["default_alpha_run"] = default_alpha_probe(sb, g, cfg)
         print(json.dumps(line))

@@ -83,6 +83,13 @@ typedef struct {
                             entries are expanded by several sampler CTAs
                             together (same results): 0 = default (32 x the
                             CTA size: eight tiles), 0xffffffff = never      */
+    uint32_t wait_polls; /* polls after which a wait between the CTAs that
+                            share a level gives up (the sample then reports
+                            SILVAN_E_TIMEOUT and the job fails; later jobs
+                            are unaffected): 0 = default (2^20, far above
+                            any real wait), 0xffffffff = no polls at all (a
+                            hook for tests of that failure path)            */
+    uint32_t pad0;
 } silvan_params_t;
 
 /* Predecessor choice of the random backtrack.  REFERENCE is the rule of
@@ -316,21 +323,25 @@ int silvan_replay_samples(silvan_graph_t g, uint64_t seed, uint32_t first, uint3
                           uint64_t ent_cap, uint64_t *ent_total);
 
 /* No counterpart in the reference.  The same per-sample sampler as
- * silvan_replay_samples, for callers that cannot allocate device memory:
- * code that records work into a CUDA graph replayed later, a process that
- * already holds its whole memory quota, or a runtime that hands the library
- * only pre-allocated buffers.  It calls no cudaMalloc/cudaFree: the sampler's
- * scratch is a fixed 64 MiB static device array (held by every GPU that loads
- * the library until exit), which limits a call to graphs of about 1.4 million
- * nodes and to 65536 samples (SILVAN_E_CAPACITY beyond).  Every output is a
- * DEVICE buffer supplied by the caller; d_records receives (node, sample,
- * count) triples, unordered, and *d_record_count their number (when it
- * exceeds record_cap the surplus is dropped and the affected samples carry
+ * silvan_replay_samples, for callers that cannot let a library allocate
+ * device memory: a process that shares the GPU under a quota it already
+ * holds in full, or a runtime that gives its libraries only buffers it
+ * allocated itself.  It calls no cudaMalloc/cudaFree or other allocating
+ * routine: the sampler's scratch is a fixed 64 MiB static device array (held
+ * by every GPU that loads the library until exit), which limits a call to
+ * graphs of at most 1,489,408 nodes and to 65536 samples (SILVAN_E_CAPACITY
+ * beyond, with the limit in silvan_last_error()).  The graph's device must
+ * be current (SILVAN_E_BADARG otherwise).  Every output is a DEVICE buffer
+ * supplied by the caller; d_records receives (node, sample, count) triples,
+ * unordered, whose sample field is the index relative to `first` (0 for
+ * sample `first`), and *d_record_count their number (when it exceeds
+ * record_cap the surplus is dropped and the affected samples carry
  * SILVAN_E_CAPACITY).  The work is queued on `stream` (a cudaStream_t, NULL
  * for the default stream); outputs are ready when the stream reaches it.  The
- * first call on a device looks up the scratch's device address and should
- * come before any stream capture.  All calls share the scratch, so calls that
- * overlap on the GPU race. */
+ * first call on a device looks up the scratch's device address (and caches
+ * it: the cache does not survive cudaDeviceReset), so it should come before
+ * any stream capture.  All calls share the scratch, so calls that overlap on
+ * the GPU race. */
 int silvan_replay_samples_noalloc(silvan_graph_t g, uint64_t seed, uint32_t first,
                                   uint32_t count, double alpha, uint32_t np_cap,
                                   int32_t *d_path_length, int32_t *d_num_paths,

@@ -21,6 +21,7 @@
 #include <set>
 #include <vector>
 #include <utility>
+#include <algorithm>
 #include <ctype.h>
 #include <unistd.h>
 #include <omp.h>
@@ -195,3 +196,87 @@ extern "C" int refbench_sample(uint32_t n, int directed, const uint64_t *out_off
 }
 
 extern "C" int refbench_max_threads() { return omp_get_max_threads(); }
+
+// ---------------------------------------------------------------------------
+// The benchmark graphs without the product library: bench.py's reference arm
+// must not load libsilvan_b200.so, so this harness carries the project's
+// seeded generators (silvan_b200/csrc/gen.cpp, compiled in by the Makefile)
+// and its own CSR build with the reference loader's semantics
+// (silvan/src/Graph.cpp:37-90: rows sorted ascending without duplicates,
+// self-loops kept, n = max id + 1, each undirected edge in both rows; for
+// directed graphs the in-rows hold the reverse edges).  The arm prints a
+// checksum of the CSR, and so does the GPU arm, so the two can be seen to
+// run on the same graph.
+// ---------------------------------------------------------------------------
+#include "gen.h"
+
+namespace {
+struct BuiltGraph {
+    uint32_t n = 0;
+    std::vector<uint64_t> out_off, in_off;
+    std::vector<uint32_t> out_adj, in_adj;
+};
+
+void csr_rows(uint32_t n, std::vector<std::pair<uint32_t, uint32_t>> &e, std::vector<uint64_t> &off,
+              std::vector<uint32_t> &adj) {
+    std::sort(e.begin(), e.end());
+    e.erase(std::unique(e.begin(), e.end()), e.end());
+    off.assign((size_t)n + 1, 0);
+    adj.resize(e.size());
+    for (size_t i = 0; i < e.size(); i++) {
+        off[e[i].first + 1]++;
+        adj[i] = e[i].second;
+    }
+    for (uint32_t i = 0; i < n; i++) off[i + 1] += off[i];
+}
+}  // namespace
+
+// kind: 0 = BA(n=a, m=b), 1 = ER(n=a, mean degree=x), 2 = R-MAT(scale=a,
+// edge factor=b, directed=c; a,b,c probabilities .57,.19,.19), 3 = grid(side=a,
+// delete fraction x, shortcut fraction y).  Returns a handle (nullptr on
+// failure) whose sizes refbench_graph_info reports.
+extern "C" void *refbench_graph_new(int kind, uint32_t a, uint32_t b, uint32_t c, double x,
+                                    double y, uint64_t seed, int directed) {
+    silvan::EdgeList e;
+    switch (kind) {
+    case 0: e = silvan::gen_ba(a, b, seed); break;
+    case 1: e = silvan::gen_er(a, x, seed); break;
+    case 2: e = silvan::gen_rmat(a, b, 0.57, 0.19, 0.19, seed, c != 0); break;
+    case 3: e = silvan::gen_grid(a, x, y, seed); break;
+    default: return nullptr;
+    }
+    BuiltGraph *g = new BuiltGraph();
+    uint32_t mx = 0;
+    for (auto &p : e) mx = std::max(mx, std::max(p.first, p.second));
+    g->n = e.empty() ? 0 : mx + 1;
+    std::vector<std::pair<uint32_t, uint32_t>> fwd, rev;
+    fwd.reserve(directed ? e.size() : 2 * e.size());
+    for (auto &p : e) {
+        fwd.push_back(p);
+        if (directed) rev.emplace_back(p.second, p.first);
+        else fwd.emplace_back(p.second, p.first);
+    }
+    csr_rows(g->n, fwd, g->out_off, g->out_adj);
+    if (directed) csr_rows(g->n, rev, g->in_off, g->in_adj);
+    return g;
+}
+
+extern "C" void refbench_graph_info(void *h, uint32_t *n, uint64_t *m_out, uint64_t *m_in) {
+    BuiltGraph *g = static_cast<BuiltGraph *>(h);
+    *n = g->n;
+    *m_out = g->out_adj.size();
+    *m_in = g->in_adj.size();
+}
+
+extern "C" void refbench_graph_csr(void *h, uint64_t *out_off, uint32_t *out_adj,
+                                   uint64_t *in_off, uint32_t *in_adj) {
+    BuiltGraph *g = static_cast<BuiltGraph *>(h);
+    std::memcpy(out_off, g->out_off.data(), sizeof(uint64_t) * g->out_off.size());
+    std::memcpy(out_adj, g->out_adj.data(), sizeof(uint32_t) * g->out_adj.size());
+    if (!g->in_off.empty()) {
+        std::memcpy(in_off, g->in_off.data(), sizeof(uint64_t) * g->in_off.size());
+        std::memcpy(in_adj, g->in_adj.data(), sizeof(uint32_t) * g->in_adj.size());
+    }
+}
+
+extern "C" void refbench_graph_free(void *h) { delete static_cast<BuiltGraph *>(h); }

@@ -60,7 +60,8 @@ class Params(C.Structure):
                 ("form", C.c_int32), ("a", C.c_double), ("seed", C.c_uint64),
                 ("verbose", C.c_double), ("np_cap", C.c_uint32), ("slots", C.c_uint32),
                 ("threads", C.c_uint32), ("block", C.c_uint32),
-                ("backtrack", C.c_uint32), ("assist_items", C.c_uint32)]
+                ("backtrack", C.c_uint32), ("assist_items", C.c_uint32),
+                ("wait_polls", C.c_uint32), ("pad0", C.c_uint32)]
 
 
 class Result(C.Structure):
@@ -375,15 +376,17 @@ class Probabilistic:
     `form` ("batched" or "plain"), `np_cap` (paths per sample), `slots` and
     `block` (sampler slots and threads per slot; 0 = chosen by the engine),
     `threads` (the divisor of union_sample; 1 = parity mode), `backtrack`
-    ("reference", or "sigma" for path-count-weighted predecessors) and
+    ("reference", or "sigma" for path-count-weighted predecessors),
     `assist_items` (BFS levels of at least this many adjacency entries are
     expanded by several sampler CTAs; 0 = 32 x the CTA size, 0xFFFFFFFF =
-    never).  Only `seed`, `backtrack` and, in top-k mode, `threads` change
-    the results."""
+    never) and `wait_polls` (polls after which a wait between CTAs that
+    share a level gives up and the job fails with E_TIMEOUT; 0 = default,
+    0xFFFFFFFF = no polls, a hook for tests of that path).  Only `seed`,
+    `backtrack` and, in top-k mode, `threads` change the results."""
 
     def __init__(self, graph: Graph, eps, delta, k=0, alpha=2.3, alpha_given=False, a=2.0,
                  m_hat=True, seed=42, form="batched", verbose=0.0, np_cap=0, slots=0,
-                 threads=1, block=0, backtrack="reference", assist_items=0):
+                 threads=1, block=0, backtrack="reference", assist_items=0, wait_polls=0):
         lib = load()
         p = Params()
         lib.silvan_params_default(C.byref(p))
@@ -393,6 +396,7 @@ class Probabilistic:
         p.form = FORM_PLAIN if form == "plain" else FORM_BATCHED
         p.np_cap, p.slots, p.threads, p.block = np_cap, slots, threads, block
         p.assist_items = assist_items
+        p.wait_polls = wait_polls
         p.backtrack = {"reference": BACKTRACK_REFERENCE,
                        "sigma": BACKTRACK_SIGMA_WEIGHTED}[backtrack]
         self.graph = graph

@@ -12,7 +12,10 @@
 // and the group is folded sequentially: lanes 0..24 each carry one Monte
 // Carlo trial, lane 25 approx, lane 26 the wimpy variance.  Different nodes
 // are independent, so the only serial work is per node.
+#include <algorithm>
 #include <cfloat>
+#include <cstring>
+#include <vector>
 
 #include "counters.cuh"
 
@@ -20,24 +23,72 @@ namespace silvan {
 
 namespace {
 
-constexpr int kScanBlocks = 296;
-constexpr int kScanThreads = 256;
+// ---------------------------------------------------------------------------
+// One commit round as a single cooperative kernel.  Its phases are separated
+// by grid-wide barriers (every CTA is resident: cooperative launch):
+//   A  the round's Rademacher signs (pass 2); records counted per node and
+//      the touched nodes listed
+//   B  per-CTA sums of the counts over a contiguous range of the list
+//   C  exclusive scan of the counts (each CTA adds the sums of the CTAs
+//      before it), the bucket offsets and the scatter cursors
+//   D  records scattered into their nodes' buckets
+//   E  buckets of at most 32 entries sorted and folded by one warp each
+//      (larger ones listed); the round's scalar sums; cursors zeroed
+//   F  buckets of more than 32 entries sorted in shared memory and folded,
+//      one CTA each
+// Each barrier is bounded: a CTA that waits longer than kBarrierPolls polls
+// records SILVAN_E_TIMEOUT in the job's error word and leaves the kernel.
+// ---------------------------------------------------------------------------
+constexpr int kCommitThreads = 1024;
+constexpr uint32_t kBarrierPolls = 1u << 22;  // far above any real wait (microseconds)
 
 __device__ __forceinline__ uint32_t round_records(const RoundBuffers &rb, const ApplyArgs &a) {
     return (uint32_t)min((uint64_t)a.n_records, rb.rec_cap);
 }
 
-// The Rademacher signs of the round's samples (pass 2), and the records per
-// node with the list of touched nodes.
-__global__ void bucket_count_kernel(const ApplyState *st) {
-    const RoundBuffers rb = st->rb;
-    const ApplyArgs a = st->a;
+__device__ __forceinline__ uint32_t ld_acquire(const uint32_t *p) {
+    uint32_t v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void st_release(uint32_t *p, uint32_t v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Grid-wide barrier over bar[0] (arrivals) and bar[1] (generation); false
+// when this CTA gave up waiting.
+__device__ bool grid_barrier(uint32_t *bar) {
+    __syncthreads();
+    int ok = 1;
+    if (threadIdx.x == 0) {
+        const uint32_t gen = ld_acquire(&bar[1]);
+        __threadfence();
+        if (atomicAdd(&bar[0], 1u) == gridDim.x - 1) {
+            bar[0] = 0u;
+            __threadfence();
+            st_release(&bar[1], gen + 1u);
+        } else {
+            uint32_t i = 0;
+            while (ld_acquire(&bar[1]) == gen) {
+                if (++i > kBarrierPolls) {
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(32);
+            }
+        }
+    }
+    return __syncthreads_and(ok) != 0;
+}
+
+__device__ void bucket_count(const RoundBuffers &rb, const ApplyArgs &a) {
+    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
     if (a.pass == 2)
-        for (uint32_t s = a.lo + blockIdx.x * blockDim.x + threadIdx.x; s < a.hi;
-             s += gridDim.x * blockDim.x)
+        for (uint32_t s = a.lo + tid; s < a.hi; s += nth)
             rb.signs[s] = rademacher_mask(a.seed, a.first_sample + s);
     const uint32_t R = round_records(rb, a);
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < R; i += gridDim.x * blockDim.x) {
+    for (uint32_t i = tid; i < R; i += nth) {
         PathRec r = rb.recs[i];
         if (r.sample < a.lo || r.sample >= a.hi) continue;
         if (atomicAdd(&rb.node_cnt[r.node], 1u) == 0u) {
@@ -47,71 +98,54 @@ __global__ void bucket_count_kernel(const ApplyState *st) {
     }
 }
 
-// Three-step exclusive scan of node_cnt over the touched list; each block owns
-// a contiguous range of the list.
+// Contiguous range of the touched list owned by this CTA.
 __device__ __forceinline__ void range_of(uint32_t T, uint32_t &b, uint32_t &e) {
     uint32_t per = (T + gridDim.x - 1) / gridDim.x;
     b = min(T, blockIdx.x * per);
     e = min(T, b + per);
 }
 
-__device__ uint32_t block_sum(uint32_t v, uint32_t *tmp) {
+__device__ void scan_reduce(const RoundBuffers &rb, uint32_t T, uint32_t *tmp) {
+    uint32_t b, e;
+    range_of(T, b, e);
+    uint32_t v = 0;
+    for (uint32_t i = b + threadIdx.x; i < e; i += blockDim.x) v += rb.node_cnt[rb.touched[i]];
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     if ((threadIdx.x & 31) == 0) tmp[threadIdx.x >> 5] = v;
     __syncthreads();
-    uint32_t t = 0;
-    if (threadIdx.x == 0) {
-        for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += tmp[w];
-        tmp[0] = t;
+    if (threadIdx.x < 32) {
+        uint32_t t = threadIdx.x < (blockDim.x >> 5) ? tmp[threadIdx.x] : 0u;
+        for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+        if (threadIdx.x == 0) rb.block_sums[blockIdx.x] = t;
     }
     __syncthreads();
-    t = tmp[0];
-    __syncthreads();
-    return t;
 }
 
-__global__ void scan_reduce_kernel(const ApplyState *st) {
-    __shared__ uint32_t tmp[32];
-    const RoundBuffers rb = st->rb;
-    const uint32_t T = *rb.n_touched;
-    uint32_t b, e;
-    range_of(T, b, e);
-    uint32_t s = 0;
-    for (uint32_t i = b + threadIdx.x; i < e; i += blockDim.x) s += rb.node_cnt[rb.touched[i]];
-    s = block_sum(s, tmp);
-    if (threadIdx.x == 0) rb.block_sums[blockIdx.x] = s;
-}
-
-// One warp: exclusive scan of the block sums, 32 at a time.
-__global__ void scan_top_kernel(const ApplyState *st, int nblocks) {
-    const RoundBuffers rb = st->rb;
-    const int lane = threadIdx.x & 31;
-    if (blockIdx.x != 0 || threadIdx.x >= 32) return;
-    uint32_t acc = 0;
-    for (int i0 = 0; i0 < nblocks; i0 += 32) {
-        const int i = i0 + lane;
-        const uint32_t v = i < nblocks ? rb.block_sums[i] : 0u;
-        uint32_t incl = v;
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += t;
-        }
-        if (i < nblocks) rb.block_sums[i] = acc + incl - v;
-        acc += __shfl_sync(0xffffffffu, incl, 31);
-    }
-    if (lane == 0) rb.block_sums[nblocks] = acc;
-}
-
-__global__ void scan_down_kernel(const ApplyState *st) {
-    __shared__ uint32_t tmp[33];
-    const RoundBuffers rb = st->rb;
-    const uint32_t T = *rb.n_touched;
-    uint32_t b, e;
-    range_of(T, b, e);
-    uint32_t carry = rb.block_sums[blockIdx.x];
+__device__ void scan_down(const RoundBuffers &rb, uint32_t T, uint32_t *tmp) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    // the sums of the CTAs before this one (warp 0), and of all CTAs
+    if (warp == 0) {
+        uint32_t before = 0, all = 0;
+        for (uint32_t i = lane; i < gridDim.x; i += 32) {
+            const uint32_t v = __ldcg(&rb.block_sums[i]);
+            all += v;
+            if (i < blockIdx.x) before += v;
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            before += __shfl_xor_sync(0xffffffffu, before, o);
+            all += __shfl_xor_sync(0xffffffffu, all, o);
+        }
+        if (lane == 0) {
+            tmp[33] = before;
+            if (blockIdx.x == gridDim.x - 1) rb.bucket_off[T] = all;
+        }
+    }
+    __syncthreads();
+    uint32_t carry = tmp[33];
+    uint32_t b, e;
+    range_of(T, b, e);
     for (uint32_t c0 = b; c0 < e; c0 += blockDim.x) {
-        uint32_t i = c0 + threadIdx.x;
+        const uint32_t i = c0 + threadIdx.x;
         uint32_t node = 0, v = 0;
         if (i < e) {
             node = rb.touched[i];
@@ -119,19 +153,20 @@ __global__ void scan_down_kernel(const ApplyState *st) {
         }
         uint32_t incl = v;
         for (int o = 1; o < 32; o <<= 1) {
-            uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+            const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
             if (lane >= o) incl += t;
         }
         if (lane == 31) tmp[warp] = incl;
         __syncthreads();
-        if (threadIdx.x == 0) {
-            uint32_t acc = 0;
-            for (int w = 0; w < nw; w++) {
-                uint32_t t = tmp[w];
-                tmp[w] = acc;
-                acc += t;
+        if (warp == 0) {
+            const uint32_t w = lane < nw ? tmp[lane] : 0u;
+            uint32_t wi = w;
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t t = __shfl_up_sync(0xffffffffu, wi, o);
+                if (lane >= o) wi += t;
             }
-            tmp[32] = acc;
+            if (lane < nw) tmp[lane] = wi - w;
+            if (lane == 31) tmp[32] = wi;
         }
         __syncthreads();
         const uint32_t excl = carry + tmp[warp] + incl - v;
@@ -142,21 +177,18 @@ __global__ void scan_down_kernel(const ApplyState *st) {
         carry += tmp[32];
         __syncthreads();
     }
-    if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) rb.bucket_off[T] = rb.block_sums[gridDim.x];
 }
 
-__global__ void bucket_scatter_kernel(const ApplyState *st) {
-    const RoundBuffers rb = st->rb;
-    const ApplyArgs a = st->a;
+__device__ void bucket_scatter(const RoundBuffers &rb, const ApplyArgs &a) {
+    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
     const uint32_t R = round_records(rb, a);
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < R; i += gridDim.x * blockDim.x) {
+    for (uint32_t i = tid; i < R; i += nth) {
         PathRec r = rb.recs[i];
         if (r.sample < a.lo || r.sample >= a.hi) continue;
         uint32_t pos = atomicAdd(&rb.node_cnt[r.node], 1u);
         rb.entries[pos] = ((unsigned long long)r.sample << 32) | r.count;
     }
 }
-
 __device__ __forceinline__ void atomic_max_nonneg_double(unsigned long long *p, double v) {
     atomicMax(p, (unsigned long long)__double_as_longlong(v));
 }
@@ -260,16 +292,22 @@ __device__ __forceinline__ void warp_bitonic_sort(unsigned long long &key) {
     }
 }
 
-constexpr int kApplyThreads = 256;
+// Shared memory of the commit kernel: phase E's per-warp buffers and phase
+// F's sort buffer share one region.
+struct SmallSmem {
+    unsigned long long buf[kCommitThreads / 32][32];
+    FoldScratch fsc[kCommitThreads / 32];
+};
+struct LargeSmem {
+    unsigned long long sbuf[kLargeBucket];
+    FoldScratch fsc;
+};
+constexpr size_t kCommitSmem = sizeof(LargeSmem) > sizeof(SmallSmem) ? sizeof(LargeSmem)
+                                                                        : sizeof(SmallSmem);
 
-// Groups of at most 32 entries: one warp per node.
-__global__ void __launch_bounds__(kApplyThreads) apply_small_kernel(const ApplyState *st) {
-    __shared__ unsigned long long buf[kApplyThreads / 32][32];
-    __shared__ FoldScratch fsc[kApplyThreads / 32];
-    const RoundBuffers rb = st->rb;
-    const JobCounters jc = st->jc;
-    const ApplyArgs a = st->a;
-    const uint32_t T = *rb.n_touched;
+// Buckets of at most 32 entries: one warp per node; larger ones are listed.
+__device__ void apply_small(const RoundBuffers &rb, const JobCounters &jc, const ApplyArgs &a,
+                            uint32_t T, SmallSmem &sm) {
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const uint32_t gw = blockIdx.x * (blockDim.x >> 5) + wib;
     const uint32_t nw = gridDim.x * (blockDim.x >> 5);
@@ -277,31 +315,27 @@ __global__ void __launch_bounds__(kApplyThreads) apply_small_kernel(const ApplyS
         const uint32_t b0 = rb.bucket_off[t];
         const uint32_t b = rb.bucket_off[t + 1] - b0;
         if (b > 32) {
-            // for apply_large, which then visits only these
             if (lane == 0) rb.large[atomicAdd(rb.n_large, 1u)] = t;
             continue;
         }
         const uint32_t node = rb.touched[t];
         unsigned long long key = (uint32_t)lane < b ? rb.entries[b0 + lane] : ~0ull;
         warp_bitonic_sort(key);
-        buf[wib][lane] = key;
+        sm.buf[wib][lane] = key;
         __syncwarp();
-        fold_node(rb, jc, a, node, b, [&](uint32_t r) { return buf[wib][r]; }, fsc[wib]);
+        fold_node(rb, jc, a, node, b, [&](uint32_t r) { return sm.buf[wib][r]; }, sm.fsc[wib]);
         __syncwarp();
     }
 }
 
-// Groups of more than 32 entries: one CTA per node, bitonic sort in shared
-// memory (groups are bounded by kLargeBucket through the sub-round size).
-__global__ void __launch_bounds__(1024) apply_large_kernel(const ApplyState *st) {
-    extern __shared__ unsigned long long sbuf[];
-    __shared__ FoldScratch fsc;
-    const RoundBuffers rb = st->rb;
-    const JobCounters jc = st->jc;
-    const ApplyArgs a = st->a;
-    const uint32_t NL = *rb.n_large;
+// Buckets of more than 32 entries: one CTA per node, a bitonic sort in shared
+// memory (buckets are bounded by kLargeBucket through the sub-round size).
+__device__ void apply_large(const RoundBuffers &rb, const JobCounters &jc, const ApplyArgs &a,
+                            LargeSmem &sm) {
+    const uint32_t NL = __ldcg(rb.n_large);
+    unsigned long long *sbuf = sm.sbuf;
     for (uint32_t li = blockIdx.x; li < NL; li += gridDim.x) {
-        const uint32_t t = rb.large[li];
+        const uint32_t t = __ldcg(&rb.large[li]);
         const uint32_t b0 = rb.bucket_off[t];
         const uint32_t b = rb.bucket_off[t + 1] - b0;
         if (b > kLargeBucket) {
@@ -331,16 +365,13 @@ __global__ void __launch_bounds__(1024) apply_large_kernel(const ApplyState *st)
         }
         if (threadIdx.x < 32) {
             const uint32_t node = rb.touched[t];
-            fold_node(rb, jc, a, node, b, [&](uint32_t r) { return sbuf[r]; }, fsc);
+            fold_node(rb, jc, a, node, b, [&](uint32_t r) { return sbuf[r]; }, sm.fsc);
         }
         __syncthreads();
     }
 }
 
-__device__ void commit_sums(const ApplyState *st) {
-    const RoundBuffers rb = st->rb;
-    const JobCounters jc = st->jc;
-    const ApplyArgs a = st->a;
+__device__ void commit_sums(const RoundBuffers &rb, const JobCounters &jc, const ApplyArgs &a) {
     unsigned long long vis = 0, cnt = 0, vd = 0, paths = 0, ball = 0, pred = 0;
     for (uint32_t s = a.lo + blockIdx.x * blockDim.x + threadIdx.x; s < a.hi;
          s += gridDim.x * blockDim.x) {
@@ -377,15 +408,78 @@ __device__ void commit_sums(const ApplyState *st) {
     }
 }
 
-// The round's scalar sums (commit_sums) and the per-node cursors zeroed for
-// the next round; neither depends on the folds.
-__global__ void commit_kernel(const ApplyState *st) {
-    commit_sums(st);
+
+__global__ void __launch_bounds__(kCommitThreads, 1) commit_round_kernel(const ApplyState *st) {
+    extern __shared__ __align__(16) unsigned char commit_smem[];
+    __shared__ uint32_t tmp[34];
     const RoundBuffers rb = st->rb;
-    const uint32_t T = *rb.n_touched;
-    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < T; t += gridDim.x * blockDim.x)
-        rb.node_cnt[rb.touched[t]] = 0;
+    const JobCounters jc = st->jc;
+    const ApplyArgs a = st->a;
+    uint32_t *bar = rb.n_touched + 2;
+    bucket_count(rb, a);
+    if (!grid_barrier(bar)) goto timeout;
+    {
+        const uint32_t T = __ldcg(rb.n_touched);
+        scan_reduce(rb, T, tmp);
+        if (!grid_barrier(bar)) goto timeout;
+        scan_down(rb, T, tmp);
+        if (!grid_barrier(bar)) goto timeout;
+        bucket_scatter(rb, a);
+        if (!grid_barrier(bar)) goto timeout;
+        apply_small(rb, jc, a, T, *reinterpret_cast<SmallSmem *>(commit_smem));
+        commit_sums(rb, jc, a);
+        // the scatter cursors back to zero for the next round
+        for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < T;
+             t += gridDim.x * blockDim.x)
+            rb.node_cnt[rb.touched[t]] = 0;
+        if (!grid_barrier(bar)) goto timeout;
+        apply_large(rb, jc, a, *reinterpret_cast<LargeSmem *>(commit_smem));
+    }
+    return;
+timeout:
+    if (threadIdx.x == 0) atomicCAS(&jc.sc->error, 0, SILVAN_E_TIMEOUT);
 }
+
+int g_commit_grid = 0;  // resident CTAs of commit_round_kernel (apply_init)
+
+}  // namespace
+
+cudaError_t apply_init() {
+    cudaError_t e = cudaFuncSetAttribute(commit_round_kernel,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)kCommitSmem);
+    if (e != cudaSuccess) return e;
+    int dev = 0, sms = 0, per_sm = 0;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess)
+        return e;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, commit_round_kernel,
+                                                      kCommitThreads, kCommitSmem);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) return cudaErrorLaunchOutOfResources;
+    g_commit_grid = sms * per_sm;
+    return cudaSuccess;
+}
+
+cudaError_t apply_round(const ApplyState *st, uint32_t *n_touched, cudaStream_t stream) {
+    if (g_commit_grid <= 0) return cudaErrorNotReady;
+    // n_touched, n_large and the barrier's two words
+    cudaError_t e = cudaMemsetAsync(n_touched, 0, 4 * sizeof(uint32_t), stream);
+    if (e != cudaSuccess) return e;
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3((unsigned)g_commit_grid);
+    cfg.blockDim = dim3(kCommitThreads);
+    cfg.dynamicSmemBytes = kCommitSmem;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, commit_round_kernel, st);
+}
+
+namespace {
 
 __global__ void stop_init_kernel(StopReduction *out, int nparts, long long init) {
     for (int i = threadIdx.x; i < nparts * kTrials; i += blockDim.x) out->mc_max[i] = init;
@@ -504,24 +598,6 @@ __global__ void peel_map_kernel(JobCounters jc, uint32_t n, const int32_t *lut, 
 
 }  // namespace
 
-cudaError_t apply_init() {
-    return cudaFuncSetAttribute(apply_large_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)(kLargeBucket * sizeof(unsigned long long)));
-}
-
-cudaError_t apply_round(const ApplyState *st, uint32_t *n_touched, cudaStream_t stream) {
-    cudaMemsetAsync(n_touched, 0, 2 * sizeof(uint32_t), stream);  // n_touched, n_large
-    bucket_count_kernel<<<592, 256, 0, stream>>>(st);
-    scan_reduce_kernel<<<kScanBlocks, kScanThreads, 0, stream>>>(st);
-    scan_top_kernel<<<1, 32, 0, stream>>>(st, kScanBlocks);
-    scan_down_kernel<<<kScanBlocks, kScanThreads, 0, stream>>>(st);
-    bucket_scatter_kernel<<<592, 256, 0, stream>>>(st);
-    apply_small_kernel<<<592, kApplyThreads, 0, stream>>>(st);
-    apply_large_kernel<<<148, 1024, kLargeBucket * sizeof(unsigned long long), stream>>>(st);
-    commit_kernel<<<148, 256, 0, stream>>>(st);
-    return cudaGetLastError();
-}
-
 __global__ void divide_kernel(const double *approx, double m, double *out, uint32_t n) {
     for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x)
         out[v] = __ddiv_rn(approx[v], m);
@@ -566,9 +642,261 @@ cudaError_t peel_map(const JobCounters &jc, uint32_t n, const int32_t *lut, int3
     return cudaGetLastError();
 }
 
-cudaError_t ranking_candidates(const JobCounters &, uint32_t, double, uint32_t *, uint32_t *,
-                               uint32_t, cudaStream_t) {
-    return cudaErrorNotSupported;
+// ---------------------------------------------------------------------------
+// Top-K selection of the ranking (see counters.cuh).  A node's key is the
+// 128-bit (approx bits, last update << 32 | node), compared as an unsigned
+// number: approx is non-negative, so its bit pattern orders like its value,
+// and node ids make every key distinct.  Digit i (i = 0 the most
+// significant) is 16 bits of it.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr uint32_t kTopkSortCap = 8192;  // candidates one CTA sorts in shared memory
+
+struct Key128 {
+    unsigned long long hi, lo;
+};
+
+__device__ __forceinline__ Key128 node_key(const JobCounters &jc, uint32_t v) {
+    Key128 k;
+    k.hi = (unsigned long long)__double_as_longlong(jc.approx[v]);
+    k.lo = ((unsigned long long)jc.last_upd[v] << 32) | v;
+    return k;
+}
+
+// word w (0 most significant) of the key
+__device__ __forceinline__ uint32_t key_word(const Key128 &k, int w) {
+    const unsigned long long x = w < 2 ? k.hi : k.lo;
+    return (w & 1) ? (uint32_t)x : (uint32_t)(x >> 32);
+}
+
+__device__ __forceinline__ uint32_t key_digit(const Key128 &k, uint32_t i) {
+    return (key_word(k, (int)(i >> 1)) >> ((i & 1) ? 0 : 16)) & 0xffffu;
+}
+
+// -1, 0, 1: the key's first L digits against the prefix's (4 words).
+__device__ __forceinline__ int cmp_prefix(const Key128 &k, const uint32_t *pre, uint32_t L) {
+    for (uint32_t w = 0; w < 4 && 2 * w < L; w++) {
+        const uint32_t mask = (2 * w + 1 < L) ? 0xffffffffu : 0xffff0000u;
+        const uint32_t a = key_word(k, (int)w) & mask, b = pre[w] & mask;
+        if (a != b) return a < b ? -1 : 1;
+    }
+    return 0;
+}
+
+// state: [0] digits fixed (L), [1..4] prefix words, [5] nodes known to be
+// above the prefix's group, [6] size of the group, [7] candidates
+__global__ void topk_hist_kernel(JobCounters jc, uint32_t n_upd, const uint32_t *state,
+                                 uint32_t *hist) {
+    const uint32_t L = state[0];
+    uint32_t pre[4] = {state[1], state[2], state[3], state[4]};
+    const int lane = threadIdx.x & 31;
+    for (uint32_t t0 = blockIdx.x * blockDim.x; t0 < n_upd; t0 += gridDim.x * blockDim.x) {
+        const uint32_t t = t0 + threadIdx.x;
+        bool in = false;
+        uint32_t d = 0;
+        if (t < n_upd) {
+            const Key128 k = node_key(jc, jc.upd_list[t]);
+            in = cmp_prefix(k, pre, L) == 0;
+            d = key_digit(k, L);
+        }
+        // one atomic per distinct digit of the warp
+        const uint32_t act = __ballot_sync(0xffffffffu, in);
+        if (in) {
+            const uint32_t peers = __match_any_sync(act, d);
+            if ((peers & ((1u << lane) - 1u)) == 0u) atomicAdd(&hist[d], (uint32_t)__popc(peers));
+        }
+    }
+}
+
+// One CTA of 1024 threads: the digit d of level L at which the K-th key lies
+// (counting from the largest), the count above it, and the state of the
+// next level (its prefix extended by d).
+__global__ void __launch_bounds__(1024) topk_pick_kernel(const uint32_t *hist, uint32_t *state,
+                                                         uint32_t K) {
+    __shared__ uint32_t ws[32];
+    __shared__ uint32_t found;
+    const uint32_t L = state[0], above = state[5];
+    const uint32_t t = threadIdx.x;
+    const int lane = t & 31, warp = t >> 5;
+    // thread t owns digits [hi - 63, hi], hi = 65535 - 64 t (descending)
+    const uint32_t top = 65535u - 64u * t;
+    uint32_t sum = 0;
+    for (int j = 0; j < 64; j++) sum += hist[top - j];
+    uint32_t incl = sum;
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t x = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += x;
+    }
+    if (lane == 31) ws[warp] = incl;
+    if (t == 0) found = 0;
+    __syncthreads();
+    if (warp == 0) {
+        const uint32_t w = ws[lane];
+        uint32_t wi = w;
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t x = __shfl_up_sync(0xffffffffu, wi, o);
+            if (lane >= o) wi += x;
+        }
+        ws[lane] = wi - w;
+    }
+    __syncthreads();
+    uint32_t before = above + ws[warp] + incl - sum;  // keys above this thread's digits
+    if (before < K && before + sum >= K) {
+        for (int j = 0; j < 64; j++) {
+            const uint32_t h = hist[top - j];
+            if (before + h >= K) {
+                const uint32_t d = top - j;
+                const uint32_t w = L >> 1;
+                state[1 + w] |= (L & 1) ? d : (d << 16);
+                state[0] = L + 1;
+                state[5] = before;
+                state[6] = h;
+                found = 1;
+                break;
+            }
+            before += h;
+        }
+    }
+    __syncthreads();
+    if (t == 0 && !found) state[0] = 0xffffffffu;  // fewer than K keys: cannot happen
+}
+
+// Every updated node whose first L digits are at least the prefix's.
+__global__ void topk_collect_kernel(JobCounters jc, uint32_t n_upd, uint32_t *state,
+                                    unsigned long long *cand, uint32_t cap) {
+    const uint32_t L = state[0];
+    uint32_t pre[4] = {state[1], state[2], state[3], state[4]};
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n_upd;
+         t += gridDim.x * blockDim.x) {
+        const Key128 k = node_key(jc, jc.upd_list[t]);
+        if (cmp_prefix(k, pre, L) >= 0) {
+            const uint32_t i = atomicAdd(&state[7], 1u);
+            if (i < cap) {
+                cand[2 * i] = k.hi;
+                cand[2 * i + 1] = k.lo;
+            }
+        }
+    }
+}
+
+// One CTA: bitonic sort of the n <= kTopkSortCap candidates, largest first,
+// in shared memory; the sorted keys go back to cand.
+__global__ void __launch_bounds__(1024) topk_sort_kernel(unsigned long long *cand,
+                                                         const uint32_t *state) {
+    extern __shared__ unsigned long long kv[];  // 2 x P words
+    const uint32_t n = state[7];
+    uint32_t P = 64;
+    while (P < n) P <<= 1;
+    for (uint32_t i = threadIdx.x; i < P; i += blockDim.x) {
+        kv[2 * i] = i < n ? cand[2 * i] : 0ull;
+        kv[2 * i + 1] = i < n ? cand[2 * i + 1] : 0ull;
+    }
+    __syncthreads();
+    for (uint32_t k = 2; k <= P; k <<= 1) {
+        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+            for (uint32_t i = threadIdx.x; i < P; i += blockDim.x) {
+                const uint32_t l = i ^ j;
+                if (l > i) {
+                    const unsigned long long ah = kv[2 * i], al = kv[2 * i + 1];
+                    const unsigned long long bh = kv[2 * l], bl = kv[2 * l + 1];
+                    const bool a_less = ah < bh || (ah == bh && al < bl);
+                    const bool desc = (i & k) == 0;
+                    if (desc ? a_less : !a_less) {
+                        kv[2 * i] = bh;
+                        kv[2 * i + 1] = bl;
+                        kv[2 * l] = ah;
+                        kv[2 * l + 1] = al;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+        cand[2 * i] = kv[2 * i];
+        cand[2 * i + 1] = kv[2 * i + 1];
+    }
+}
+
+}  // namespace
+
+uint32_t topk_capacity(uint32_t K) { return std::max<uint32_t>(kTopkSortCap, 2u * K); }
+
+int topk_select(const JobCounters &jc, uint32_t n_upd, uint32_t K, const TopkBuffers &tb,
+                cudaStream_t stream, uint32_t *nodes, double *values, uint32_t *count) {
+    *count = 0;
+    if (n_upd == 0 || K == 0) return SILVAN_OK;
+    if (tb.cap < topk_capacity(K)) return SILVAN_E_BADARG;
+    static bool attr_set = false;  // the sort kernel's shared memory (once per process)
+    if (!attr_set) {
+        if (cudaFuncSetAttribute(topk_sort_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(2 * kTopkSortCap * sizeof(unsigned long long))) !=
+            cudaSuccess)
+            return SILVAN_E_CUDA;
+        attr_set = true;
+    }
+    uint32_t *hs = tb.h_state;
+    for (int i = 0; i < 8; i++) hs[i] = 0;
+    if (cudaMemcpyAsync(tb.state, hs, 8 * sizeof(uint32_t), cudaMemcpyHostToDevice, stream) !=
+        cudaSuccess)
+        return SILVAN_E_CUDA;
+    // refine while the candidates (keys at or above the prefix) would not fit
+    uint32_t ncand = n_upd;
+    while (ncand > tb.cap) {
+        if (cudaMemsetAsync(tb.hist, 0, 65536 * sizeof(uint32_t), stream) != cudaSuccess)
+            return SILVAN_E_CUDA;
+        topk_hist_kernel<<<592, 256, 0, stream>>>(jc, n_upd, tb.state, tb.hist);
+        topk_pick_kernel<<<1, 1024, 0, stream>>>(tb.hist, tb.state, K);
+        if (cudaMemcpyAsync(hs, tb.state, 8 * sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                            stream) != cudaSuccess ||
+            cudaStreamSynchronize(stream) != cudaSuccess)
+            return SILVAN_E_CUDA;
+        if (hs[0] > 8) return SILVAN_E_STATE;
+        ncand = hs[5] + hs[6];
+        if (hs[0] == 8 && ncand > tb.cap) return SILVAN_E_STATE;  // keys are distinct
+    }
+    topk_collect_kernel<<<592, 256, 0, stream>>>(jc, n_upd, tb.state, tb.cand, tb.cap);
+    if (cudaMemcpyAsync(hs, tb.state, 8 * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(stream) != cudaSuccess)
+        return SILVAN_E_CUDA;
+    const uint32_t n = hs[7];
+    if (n > tb.cap || n < std::min(K, n_upd)) return SILVAN_E_STATE;
+    const uint32_t take = std::min(K, n);
+    if (n <= kTopkSortCap) {
+        topk_sort_kernel<<<1, 1024, 2 * kTopkSortCap * sizeof(unsigned long long), stream>>>(
+            tb.cand, tb.state);
+        if (cudaMemcpyAsync(tb.h_cand, tb.cand, 2 * sizeof(unsigned long long) * take,
+                            cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
+            cudaStreamSynchronize(stream) != cudaSuccess)
+            return SILVAN_E_CUDA;
+    } else {
+        // more than one CTA sorts: the (at most 2K) candidates are ordered on
+        // the host, still without any n-sized transfer
+        if (cudaMemcpyAsync(tb.h_cand, tb.cand, 2 * sizeof(unsigned long long) * n,
+                            cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
+            cudaStreamSynchronize(stream) != cudaSuccess)
+            return SILVAN_E_CUDA;
+        std::vector<uint32_t> ord(n);
+        for (uint32_t i = 0; i < n; i++) ord[i] = i;
+        const unsigned long long *c = tb.h_cand;
+        std::partial_sort(ord.begin(), ord.begin() + take, ord.end(), [&](uint32_t x, uint32_t y) {
+            return c[2 * x] != c[2 * y] ? c[2 * x] > c[2 * y] : c[2 * x + 1] > c[2 * y + 1];
+        });
+        std::vector<unsigned long long> tmp(2 * (size_t)take);
+        for (uint32_t i = 0; i < take; i++) {
+            tmp[2 * i] = c[2 * ord[i]];
+            tmp[2 * i + 1] = c[2 * ord[i] + 1];
+        }
+        std::copy(tmp.begin(), tmp.end(), tb.h_cand);
+    }
+    for (uint32_t i = 0; i < take; i++) {
+        nodes[i] = (uint32_t)tb.h_cand[2 * i + 1];
+        std::memcpy(&values[i], &tb.h_cand[2 * i], sizeof(double));
+    }
+    *count = take;
+    return SILVAN_OK;
 }
 
 }  // namespace silvan

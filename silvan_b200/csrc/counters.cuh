@@ -46,7 +46,7 @@ struct RoundBuffers {
     // bucketing by node
     uint32_t *node_cnt;      // n, zero between rounds
     uint32_t *touched;       // distinct nodes of the round
-    uint32_t *n_touched;
+    uint32_t *n_touched;     // [0] touched nodes, [1] large buckets, [2..3] grid barrier
     uint32_t *bucket_off;    // n_touched + 1
     uint32_t *large;         // buckets of more than 32 entries (listed by apply_small)
     uint32_t *n_large;       // = n_touched + 1 (both zeroed together)
@@ -88,15 +88,18 @@ struct ApplyState {
     ApplyArgs a;
 };
 
-// Kernels apply_round launches (one fewer in pass 1: no Rademacher signs).
-constexpr int kApplyRoundKernels = 10;
+// Kernels apply_round launches: one cooperative kernel (after a memset).
+constexpr int kApplyRoundKernels = 1;
 
 // Commits round-local samples [a.lo, a.hi) of the round buffers to the job
-// counters, all read from `st` on the device.  Launches only, with fixed grid
-// sizes, so the sequence can be captured in a CUDA graph.  n_touched is the
-// RoundBuffers field of the same struct (passed separately for the memset).
+// counters, all read from `st` on the device: one cooperative kernel whose
+// phases are separated by grid-wide barriers.  Launches only, with a fixed
+// grid, so it can be captured in a CUDA graph.  n_touched is the RoundBuffers
+// field of the same struct (4 words: touched nodes, large buckets and the
+// grid barrier's two words, zeroed here before the kernel).
 cudaError_t apply_round(const ApplyState *st, uint32_t *n_touched, cudaStream_t stream);
-// One-time function attributes of the apply kernels (call before capturing).
+// Function attributes and resident grid of the commit kernel on the current
+// device (call before capturing).
 cudaError_t apply_init();
 
 // Reduction for one stopping-rule evaluation: per partition and trial the
@@ -130,12 +133,32 @@ cudaError_t peel_map(const JobCounters &jc, uint32_t n, const int32_t *lut, int3
 cudaError_t peel_hist(const JobCounters &jc, uint32_t n, int32_t idx_min, int32_t nbins,
                       uint32_t *hist, cudaStream_t stream);
 
-// Top-(k+1) value of approx (top-k mode, Probabilistic.cpp:949) is computed on
-// the host from the ranking; the ranking itself:
-//   order by (approx desc, last update desc, node desc), never-updated nodes
-//   after all updated ones in ascending id (the initial Ranking_list).
-cudaError_t ranking_candidates(const JobCounters &jc, uint32_t n, double threshold,
-                               uint32_t *out_nodes, uint32_t *out_count, uint32_t cap,
-                               cudaStream_t stream);
+// Ranking of the top-k mode (the reference's Ranking_list,
+// silvan/src/Ranking_list.cpp:20-43, as Probabilistic.cpp:587-687 reads it):
+// nodes ordered by (approx desc, last update desc, node desc) -- a node that
+// reaches a value later is put before the nodes that reached it earlier, and
+// within one sample the larger id is the later update -- with the
+// never-updated nodes after all updated ones in ascending id.
+//
+// topk_select finds the K best updated nodes on the device: the 128-bit keys
+// (approx bits, last update << 32 | node) of the updated nodes (upd_list) are
+// radix-selected 16 bits at a time (a histogram per level; a level is refined
+// only while its boundary group is too large), the candidates are compacted
+// and sorted by one CTA in shared memory (or on the host when K is larger than
+// that CTA's buffer), so only the K winners cross to the host.
+struct TopkBuffers {
+    uint32_t *hist = nullptr;            // 65536 bins
+    uint32_t *state = nullptr;           // device selection state (8 words)
+    unsigned long long *cand = nullptr;  // 2 x cap words: keys (hi, lo)
+    uint32_t cap = 0;                    // candidate capacity
+    uint32_t *h_state = nullptr;         // pinned copy of state
+    unsigned long long *h_cand = nullptr;  // pinned, 2 x cap words
+};
+// Candidate capacity for a selection of K.
+uint32_t topk_capacity(uint32_t K);
+// The K best updated nodes (fewer when fewer were updated), best first, with
+// their approx values.  n_upd is the number of entries of jc.upd_list.
+int topk_select(const JobCounters &jc, uint32_t n_upd, uint32_t K, const TopkBuffers &tb,
+                cudaStream_t stream, uint32_t *nodes, double *values, uint32_t *count);
 
 }  // namespace silvan

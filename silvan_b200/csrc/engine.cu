@@ -1,5 +1,6 @@
 // Host engine (see engine.h).
 #include "engine.h"
+#include "components.h"
 
 #include <algorithm>
 #include <atomic>
@@ -267,12 +268,15 @@ int DeviceGraph::upload() {
 }
 
 int DeviceGraph::finish_from_host_copy() {
+    // The component numbers are the completion order of the reference's
+    // sequential depth-first search (the host copy of the out-rows); the
+    // diameter bound over them runs on the device.
     const double t0 = now_seconds();
     ncomp = compute_scc(host, cc);
-    diameter = estimate_diameter(host, cc, ncomp);
-    diameter_seconds = now_seconds() - t0;
     RK(dmalloc(&d_cc, n));
     CK(cudaMemcpy(d_cc, cc.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice));
+    RK(device_directed_bound(*this, cudaStreamLegacy));
+    diameter_seconds = now_seconds() - t0;
     return SILVAN_OK;
 }
 
@@ -662,11 +666,18 @@ int Engine::round(const std::vector<Job *> &jobs, const std::vector<JobRequest> 
         fill(s, idx[s], total);
         total += r.count;
     }
+    // the round's wait limit: the smallest any of its jobs asks for
+    uint32_t polls = kDefaultWaitPolls;
+    for (uint32_t i : idx) {
+        const uint32_t w = jobs[i]->params().wait_polls;
+        polls = std::min(polls, w == 0u ? kDefaultWaitPolls : (w == 0xffffffffu ? 0u : w));
+    }
     h_hdr_->nsegs = (uint32_t)idx.size();
     h_hdr_->total = total;
     h_hdr_->work = 0;
     h_hdr_->cycles = 0;
     h_hdr_->max_cycles = 0;
+    h_hdr_->wait_polls = polls;
     const int block = choose_block(jobs, reqs, idx, total);
     int bi = -1;
     for (int b = 0; b < kNB; b++)
@@ -691,6 +702,23 @@ int Engine::round(const std::vector<Job *> &jobs, const std::vector<JobRequest> 
                            cudaMemcpyDeviceToHost, stream_));
         CK(cudaMemcpyAsync(h_hdr_, d_hdr_, sizeof(RoundHeader), cudaMemcpyDeviceToHost, stream_));
         CK(cudaStreamSynchronize(stream_));
+        if (h_hdr_->failed > 0 || h_hdr_->finished < total) {
+            // A shared level gave up a wait: its records may be left
+            // non-neutral and the CTAs that owned them left the launch.  Every
+            // slot is re-initialised (the launch has ended, so nothing writes
+            // to them any more) before any later round uses it.  The samples
+            // concerned carry SILVAN_E_TIMEOUT into their jobs' commits; if
+            // samples were left undrawn, the whole round fails.
+            CK(sampler_init_slots(slots_.rec, slots_.hits, (uint64_t)slots_.slots * slots_.n,
+                                  stream_));
+            CK(cudaStreamSynchronize(stream_));
+            slot_resets_++;
+            if (h_hdr_->finished < total) {
+                set_error("sampler round ended with samples undrawn (waits between CTAs "
+                          "that share a level gave up)");
+                return SILVAN_E_TIMEOUT;
+            }
+        }
         float ms = 0;
         cudaEventElapsedTime(&ms, ev_[0], ev_[1]);
         sample_ms_ += ms;
@@ -736,6 +764,7 @@ int Engine::round(const std::vector<Job *> &jobs, const std::vector<JobRequest> 
         h_hdr_->work = 0;
         h_hdr_->cycles = 0;
         h_hdr_->max_cycles = 0;
+        h_hdr_->wait_polls = polls;
     }
     for (uint32_t s = 0; s < idx.size(); s++) records[idx[s]] = h_cursors_[s];
     return SILVAN_OK;
@@ -883,6 +912,11 @@ Job::~Job() {
     dfree(d_nunc_);
     dfree(d_lut_);
     dfree(d_hist_);
+    dfree(tk_.hist);
+    dfree(tk_.state);
+    dfree(tk_.cand);
+    hfree(tk_.h_state);
+    hfree(tk_.h_cand);
     hfree(h_state_);
     hfree(h_red_);
     hfree(h_sc_);
@@ -904,7 +938,7 @@ int Job::alloc_round(uint32_t max_samples, uint64_t rec_cap) {
     RK(dmalloc(&r.ball, max_samples));
     RK(dmalloc(&r.pred, max_samples));
     RK(dmalloc(&r.node_cnt, n_));
-    RK(dmalloc(&r.n_touched, 2));
+    RK(dmalloc(&r.n_touched, 4));
     r.n_large = r.n_touched + 1;
     RK(dmalloc(&r.block_sums, 1024));
     r.rec_cursor = nullptr;
@@ -1051,7 +1085,10 @@ int Job::sync_scalars(JobScalars &sc) {
                            : sc.error == SILVAN_E_NP_CAP
                                ? "a sample asked for more shortest paths than the job's cap"
                            : sc.error == SILVAN_E_CAPACITY ? "a per-sample buffer overflowed"
-                                                           : "device sampler inconsistency";
+                           : sc.error == SILVAN_E_TIMEOUT
+                               ? "a bounded wait between GPU thread blocks gave up (a BFS level "
+                                 "shared between CTAs, or a grid barrier of the commit)"
+                               : "device sampler inconsistency";
         set_error(what);
         return sc.error;
     }
@@ -1159,36 +1196,42 @@ int Job::peel(double a, bool enabled) {
 }
 
 // Current ranking list (silvan/src/Ranking_list.cpp): the union_sample nodes
-// of largest (approx, last update), never-updated nodes after the updated
-// ones in ascending id.
+// of largest (approx, last update, id), selected on the device; the
+// never-updated nodes of the initial list (ids < union_sample, ascending)
+// after the updated ones.
 int Job::ranking(std::vector<uint32_t> &el, std::vector<double> &val) {
-    const uint32_t n = n_;
-    std::vector<double> ap(n);
-    std::vector<uint32_t> lu(n);
-    CK(cudaMemcpyAsync(ap.data(), jc_.approx, sizeof(double) * n, cudaMemcpyDeviceToHost,
-                       stream_));
-    CK(cudaMemcpyAsync(lu.data(), jc_.last_upd, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost,
-                       stream_));
-    CK(cudaStreamSynchronize(stream_));
     const uint32_t K = union_sample_;
-    std::vector<uint32_t> idx;
-    idx.reserve(n);
-    for (uint32_t i = 0; i < n; i++)
-        if (lu[i] != 0) idx.push_back(i);
-    auto better = [&](uint32_t x, uint32_t y) {
-        if (ap[x] != ap[y]) return ap[x] > ap[y];
-        if (lu[x] != lu[y]) return lu[x] > lu[y];
-        return x > y;  // same sample: ascending node order, later node is newer
-    };
-    const size_t take = std::min<size_t>(K, idx.size());
-    std::partial_sort(idx.begin(), idx.begin() + take, idx.end(), better);
-    idx.resize(take);
-    // never-updated nodes of the initial list (ids < K) fill the tail
-    for (uint32_t i = 0; i < K && idx.size() < K; i++)
-        if (lu[i] == 0) idx.push_back(i);
-    el = idx;
-    val.resize(el.size());
-    for (size_t i = 0; i < el.size(); i++) val[i] = ap[el[i]];
+    if (!tk_.hist) {
+        tk_.cap = topk_capacity(K);
+        RK(dmalloc(&tk_.hist, 65536));
+        RK(dmalloc(&tk_.state, 8));
+        RK(dmalloc(&tk_.cand, 2 * (uint64_t)tk_.cap));
+        RK(hmalloc(&tk_.h_state, 8));
+        RK(hmalloc(&tk_.h_cand, 2 * (uint64_t)tk_.cap));
+    }
+    JobScalars sc;
+    CK(cudaMemcpyAsync(h_sc_, jc_.sc, sizeof(JobScalars), cudaMemcpyDeviceToHost, stream_));
+    CK(cudaStreamSynchronize(stream_));
+    sc = *h_sc_;
+    el.resize(K);
+    val.resize(K);
+    uint32_t cnt = 0;
+    RK(topk_select(jc_, sc.n_upd, K, tk_, stream_, el.data(), val.data(), &cnt));
+    el.resize(cnt);
+    val.resize(cnt);
+    if (cnt < K) {
+        // never-updated nodes of the initial list (ids < K) fill the tail
+        const uint32_t m = std::min(K, n_);
+        std::vector<uint32_t> lu(m);
+        CK(cudaMemcpyAsync(lu.data(), jc_.last_upd, sizeof(uint32_t) * m, cudaMemcpyDeviceToHost,
+                           stream_));
+        CK(cudaStreamSynchronize(stream_));
+        for (uint32_t i = 0; i < m && el.size() < K; i++)
+            if (lu[i] == 0) {
+                el.push_back(i);
+                val.push_back(0.0);
+            }
+    }
     return SILVAN_OK;
 }
 

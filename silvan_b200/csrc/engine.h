@@ -139,6 +139,8 @@ class Engine {
     uint32_t sampler_launches() const { return sampler_launches_; }
     uint32_t assisted_levels() const { return assisted_levels_; }
     uint64_t helper_tiles() const { return helper_tiles_; }
+    // times every slot was re-initialised after a shared level gave up a wait
+    uint32_t slot_resets() const { return slot_resets_; }
     // Shortens the requests of a multi-job round so that the round's
     // predicted CTA time fits `round_ms` on the resident slots: jobs that
     // need little get all of it, the rest share what is left evenly (every
@@ -182,6 +184,7 @@ class Engine {
     uint32_t sampler_launches_ = 0;
     uint32_t assisted_levels_ = 0;  // BFS levels expanded with the help board
     uint64_t helper_tiles_ = 0;     // tiles of those levels done by helping CTAs
+    uint32_t slot_resets_ = 0;
     cudaEvent_t ev_[4] = {nullptr, nullptr, nullptr, nullptr};
     float sample_ms_ = 0;
     uint64_t launches_ = 0;
@@ -285,6 +288,7 @@ class Job {
     uint32_t *d_unc_ = nullptr, *d_nunc_ = nullptr;
     int32_t *d_lut_ = nullptr;
     uint32_t *d_hist_ = nullptr;
+    TopkBuffers tk_{};  // top-k mode: device selection of the ranking
     cudaEvent_t ev_run_[2] = {nullptr, nullptr};
     FILE *sink_ = nullptr;
     std::string out_;  // pending status lines

@@ -218,11 +218,18 @@ uint32_t estimate_diameter(const HostGraph &g, const std::vector<uint32_t> &cc, 
         }
         return (uint32_t)dist[q[tail - 1]];
     };
-    std::vector<uint32_t> ecc_f(ncomp), ecc_b(ncomp), ecc_fp(ncomp);
+    std::vector<uint32_t> ecc_f(ncomp), ecc_b(ncomp);
     for (uint32_t c = 0; c < ncomp; c++) {
         ecc_f[c] = ecc(pivot[c], false, dist_f);
         ecc_b[c] = ecc(pivot[c], true, dist_b);
     }
+    return diameter_recursion(g, cc, ncomp, ecc_f, ecc_b);
+}
+
+uint32_t diameter_recursion(const HostGraph &g, const std::vector<uint32_t> &cc, uint32_t ncomp,
+                            const std::vector<uint32_t> &ecc_f, const std::vector<uint32_t> &ecc_b) {
+    const uint32_t n = g.n;
+    std::vector<uint32_t> ecc_fp(ncomp);
     // Components complete in reverse topological order, so every edge between
     // components goes to a smaller id and the DP below (Graph.cpp:298-306) can
     // run in ascending id order over the edges of each component.

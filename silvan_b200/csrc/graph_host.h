@@ -57,5 +57,9 @@ uint32_t compute_scc(const HostGraph &g, std::vector<uint32_t> &cc);
 
 // AllCCUpperBound diameter bound (silvan/src/Graph.cpp:205-316).
 uint32_t estimate_diameter(const HostGraph &g, const std::vector<uint32_t> &cc, uint32_t ncomp);
+// The AllCCUpperBound recursion over the condensation (Graph.cpp:298-306)
+// from every component's forward and backward pivot eccentricity.
+uint32_t diameter_recursion(const HostGraph &g, const std::vector<uint32_t> &cc, uint32_t ncomp,
+                            const std::vector<uint32_t> &ecc_f, const std::vector<uint32_t> &ecc_b);
 
 }  // namespace silvan

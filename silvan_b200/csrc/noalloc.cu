@@ -1,25 +1,29 @@
 // silvan_replay_samples_noalloc: the per-sample sampler with its scratch in a
 // fixed device array, for callers that must not allocate device memory.
 //
-// Who needs it.  Code that runs where cudaMalloc is unavailable or forbidden:
-// a caller that records work into a CUDA graph it replays later (allocation
-// addresses must stay fixed), a host process sharing the GPU under a strict
-// memory quota that already owns all the memory it may use, or an embedding
-// runtime that hands the library only pre-allocated buffers.  The regular
-// entry points allocate the sampler slots (tens of MB per slot) and the round
-// buffers on first use; this one uses only the array below plus the buffers
-// the caller passes.
+// Who needs it.  Some callers cannot let a library allocate GPU memory: a
+// process that shares the GPU under a strict quota and already holds all the
+// memory it may use, or a runtime (a framework's memory pool, an embedding
+// host) that hands its libraries only buffers it allocated itself and
+// forbids allocation calls behind its back.  The regular entry points
+// allocate the sampler slots (tens of MB per slot) and the round buffers on
+// first use; this one uses only the array below plus the buffers the caller
+// passes, and calls no allocating routine.
 //
 // The scratch is a file-scope static __device__ array of kScratchBytes
 // (64 MiB), held by every GPU that loads the library until the process exits.
 // Host code must not pass the array's name to a kernel: on the host it is a
 // stand-in symbol, not a device address.  The device address is taken once per
 // device, with that device current, by cudaGetSymbolAddress during the first
-// call on that device; that first call should therefore come before any stream
-// capture.  All calls share the array and it keeps the previous call's
-// contents, so every call re-initialises the part it uses; calls that overlap
-// on the GPU (different streams, or different host threads) race on it.
+// call on that device, and cached; that first call should therefore come
+// before any stream capture.  The cached address does not survive a
+// cudaDeviceReset (a process that resets a device must not call this entry
+// point on it again).  All calls share the array and it keeps the previous
+// call's contents, so every call re-initialises the part it uses; calls that
+// overlap on the GPU (different streams, or different host threads) race on
+// it.
 #include <mutex>
+#include <string>
 
 #include "engine.h"
 #include "sampler.cuh"
@@ -70,7 +74,18 @@ __global__ void noalloc_setup_kernel(RoundHeader *hdr, SegDesc *seg, RoundHeader
     }
 }
 
-size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+constexpr size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+// Scratch layout: header | segment | ball[kMaxSamples] | pred[kMaxSamples] |
+// slots.  A slot takes a node record and three u32 words per node, the
+// meeting-edge list and its prefix, and up to 256 bytes of alignment for
+// each of its six arrays.
+constexpr size_t kHeadBytes = align256(sizeof(RoundHeader)) + align256(sizeof(SegDesc)) +
+                              2 * align256(sizeof(uint32_t) * kMaxSamples);
+constexpr size_t kSlotBytesPerNode = sizeof(NodeRec) + 3 * sizeof(uint32_t);
+constexpr size_t kSlotFixedBytes = (sizeof(uint2) + sizeof(uint64_t)) * kMeetCap + 6 * 256;
+// largest graph for which one slot fits
+constexpr uint64_t kMaxNodes = (kScratchBytes - kHeadBytes - kSlotFixedBytes) / kSlotBytesPerNode;
 
 }  // namespace
 
@@ -89,10 +104,19 @@ int replay_samples_noalloc(const DeviceGraph &G, uint64_t seed, uint32_t first, 
         set_error("silvan_replay_samples_noalloc draws at most 65536 samples per call");
         return SILVAN_E_CAPACITY;
     }
+    {
+        int cur = -1;
+        if (cudaGetDevice(&cur) != cudaSuccess || cur != G.device) {
+            cudaGetLastError();
+            set_error("silvan_replay_samples_noalloc must run with the graph's device current "
+                      "(the scratch is per device)");
+            return SILVAN_E_BADARG;
+        }
+    }
     unsigned char *base = nullptr;
     int rc = scratch_address(&base);
     if (rc != SILVAN_OK) return rc;
-    // scratch layout: header | segment | ball[count] | pred[count] | slots
+    // scratch layout (kHeadBytes, then the slots)
     const uint64_t n = G.n;
     size_t off = 0;
     RoundHeader *hdr = (RoundHeader *)(base + off);
@@ -103,13 +127,14 @@ int replay_samples_noalloc(const DeviceGraph &G, uint64_t seed, uint32_t first, 
     off += align256(sizeof(uint32_t) * kMaxSamples);
     uint32_t *pred = (uint32_t *)(base + off);
     off += align256(sizeof(uint32_t) * kMaxSamples);
-    const size_t per_slot = sizeof(NodeRec) * n + 3 * sizeof(uint32_t) * n +
-                            (sizeof(uint2) + sizeof(uint64_t)) * kMeetCap + 5 * 256;
+    const size_t per_slot = kSlotBytesPerNode * n + kSlotFixedBytes;
     const size_t avail = kScratchBytes - off;
     uint64_t slots = avail / per_slot;
     if (slots == 0) {
-        set_error("graph too large for the fixed sampler scratch of "
-                  "silvan_replay_samples_noalloc (64 MiB: about 1.4 million nodes)");
+        set_error("graph of " + std::to_string(n) +
+                  " nodes too large for the fixed sampler scratch of "
+                  "silvan_replay_samples_noalloc (64 MiB: at most " +
+                  std::to_string(kMaxNodes) + " nodes)");
         return SILVAN_E_CAPACITY;
     }
     int dev = 0, sms = 0;
@@ -158,7 +183,10 @@ int replay_samples_noalloc(const DeviceGraph &G, uint64_t seed, uint32_t first, 
     sd.recs = reinterpret_cast<PathRec *>(d_records);
     sd.rec_cursor = d_record_count;
     sd.rec_cap = record_cap;
-    RoundHeader h{1u, count, 0u, 0u};
+    RoundHeader h{};
+    h.nsegs = 1u;
+    h.total = count;
+    h.wait_polls = kDefaultWaitPolls;
     SamplerLaunch L{};
     L.slots = S;
     L.hdr = hdr;

@@ -91,6 +91,8 @@ struct SamplerSmem {
     uint32_t a_tile;   // the tile this CTA took
     uint32_t a_ok;     // the tile's waits ended
     uint32_t a_drained, a_polls, a_nap;  // no sample left; board polls since; next nap (ns)
+    uint32_t a_spin;    // polls of a bounded wait (RoundHeader::wait_polls)
+    uint32_t a_leave;   // a shared level of this CTA's sample failed: take no more samples
 };
 
 __device__ __forceinline__ uint32_t lanemask_lt() {
@@ -525,11 +527,14 @@ __device__ void expand_level(const SegDesc &A, SamplerSmem<BLOCK> &s, NodeRec *r
 //     tiles, in item order within the tile.
 // The items, keys, joins and append order are those of expand_level, so the
 // level's result is bit-identical.  Tiles are taken in order and no tile
-// waits for a later one, so every wait ends; each is bounded all the same: a
-// wait that gives up marks the level failed (the sample reports
-// SILVAN_E_TIMEOUT) and the tile skips its writes.
+// waits for a later one, so every wait ends; each is bounded all the same
+// (RoundHeader::wait_polls polls): a wait that gives up marks the level
+// failed (the sample reports SILVAN_E_TIMEOUT) and the tile skips its
+// writes.  Records that the failed level touched may then be left
+// non-neutral, and helpers may still be writing to them, so the owner's CTA
+// takes no further sample in the launch and the host re-initialises the
+// slots before the next one.
 // ---------------------------------------------------------------------------
-constexpr uint32_t kAssistSpin = 1u << 20;   // polls of a bounded wait (>= 0.1 s)
 constexpr uint32_t kAssistPolls = 1u << 18;  // board polls of a CTA without samples
 constexpr unsigned long long kCntMask = (1ull << 31) - 1u;
 
@@ -561,8 +566,8 @@ __device__ __forceinline__ unsigned long long cnt_word(uint32_t state, unsigned 
 }
 
 // Thread 0: waits until *p == 0 (false: gave up).
-__device__ bool wait_zero(const uint32_t *p) {
-    for (uint32_t i = 0; i < kAssistSpin; i++) {
+__device__ bool wait_zero(const uint32_t *p, uint32_t limit) {
+    for (uint32_t i = 0; i < limit; i++) {
         if (ld_acquire_u32(p) == 0u) return true;
         __nanosleep(128);
     }
@@ -570,8 +575,8 @@ __device__ bool wait_zero(const uint32_t *p) {
 }
 
 // Thread 0: waits until *p >= v (false: gave up).
-__device__ bool wait_at_least(const uint32_t *p, uint32_t v) {
-    for (uint32_t i = 0; i < kAssistSpin; i++) {
+__device__ bool wait_at_least(const uint32_t *p, uint32_t v, uint32_t limit) {
+    for (uint32_t i = 0; i < limit; i++) {
         if (ld_acquire_u32(p) >= v) return true;
         __nanosleep(128);
     }
@@ -581,10 +586,11 @@ __device__ bool wait_at_least(const uint32_t *p, uint32_t v) {
 // Warp 0: waits until the phase 1 of every tile before t is done.  hit_flag
 // of a tile is 1 once its own hits are recorded and 2 once those of every
 // tile up to it are; the warp reads 32 predecessors at a time.
-__device__ bool lookback_hits(const uint32_t *hit_flag, uint32_t t) {
+__device__ bool lookback_hits(const uint32_t *hit_flag, uint32_t t, uint32_t limit) {
     const uint32_t lane = threadIdx.x & 31;
     uint32_t j = t;
-    for (uint32_t spin = 0; spin < kAssistSpin;) {
+    if (j == 0) return true;
+    for (uint32_t spin = 0; spin < limit;) {
         if (j == 0) return true;
         const uint32_t f = lane < j ? ld_acquire_u32(&hit_flag[j - 1 - lane]) : 2u;
         const uint32_t m2 = __ballot_sync(0xffffffffu, f == 2u);
@@ -604,11 +610,12 @@ __device__ bool lookback_hits(const uint32_t *hit_flag, uint32_t t) {
 // Warp 0: sums of the joins and meeting edges of the tiles before t (the
 // decoupled look-back of a single-pass scan).  The same in every lane.
 __device__ bool lookback_counts(const unsigned long long *cnt_flag, uint32_t t,
-                                unsigned long long &ej, unsigned long long &em) {
+                                unsigned long long &ej, unsigned long long &em, uint32_t limit) {
     const uint32_t lane = threadIdx.x & 31;
     uint32_t j = t;
     ej = em = 0;
-    for (uint32_t spin = 0; spin < kAssistSpin;) {
+    if (j == 0) return true;
+    for (uint32_t spin = 0; spin < limit;) {
         if (j == 0) return true;
         const unsigned long long w =
             lane < j ? ld_acquire_u64(&cnt_flag[j - 1 - lane]) : cnt_word(2u, 0, 0);
@@ -806,7 +813,7 @@ __device__ void assist_tile(SamplerSmem<BLOCK> &s, const AssistBoard &B, uint32_
             st_release_u32(&hit_flag[t], 1u);
         }
         __syncwarp();
-        const bool ok = lookback_hits(hit_flag, t);
+        const bool ok = lookback_hits(hit_flag, t, s.a_spin);
         if (lane == 0) {
             // published even after a failed wait, so that later tiles do not
             // wait as well (the level is reported failed)
@@ -873,7 +880,7 @@ __device__ void assist_tile(SamplerSmem<BLOCK> &s, const AssistBoard &B, uint32_
         bool ok = true;
         if (t > 0) {
             __syncwarp();
-            ok = lookback_counts(cnt_flag, t, ej, em);
+            ok = lookback_counts(cnt_flag, t, ej, em, s.a_spin);
             if (lane == 0) st_release_u64(&cnt_flag[t], cnt_word(2u, ej + aj, em + am));
         }
         ok = ok && s.a_ok != 0u;
@@ -1071,7 +1078,7 @@ __device__ bool expand_level_assisted(const SamplerLaunch &L, const SegDesc &A,
     if (!fits) return false;
     assist_work<BLOCK>(s, L, e, true);
     if (threadIdx.x == 0) {
-        const bool ok = wait_at_least(&E->done, tcarry);
+        const bool ok = wait_at_least(&E->done, tcarry, s.a_spin);
         __threadfence();
         if (ok && __ldcg(&E->err) == 0u) {
             const AssistLevel &V = s.lvl;
@@ -1086,14 +1093,20 @@ __device__ bool expand_level_assisted(const SamplerLaunch &L, const SegDesc &A,
         } else {
             s.status = SILVAN_E_TIMEOUT;
             s.sum_new = 0u;
+            s.a_leave = 1u;
         }
         // hand the entry on only when no helper is inside any more: a helper
         // either shows in `inside` here or sees the closed state and leaves
         atomicAnd(&L.hdr->open_mask, ~(1u << e));
         atomicExch(&E->state, (s.a_state & ~3u) | 3u);
         __threadfence();
-        if (wait_zero(&E->inside)) st_release_u32(&E->state, ((s.a_state >> 2) + 1u) << 2);
-        else if (s.status == 0) s.status = SILVAN_E_TIMEOUT;  // the entry stays closed
+        if (wait_zero(&E->inside, s.a_spin)) {
+            st_release_u32(&E->state, ((s.a_state >> 2) + 1u) << 2);
+        } else {
+            // the entry stays closed until the next launch reopens it
+            if (s.status == 0) s.status = SILVAN_E_TIMEOUT;
+            s.a_leave = 1u;
+        }
     }
     return true;
 }
@@ -1133,11 +1146,15 @@ __global__ void __launch_bounds__(BLOCK, Shape<BLOCK>::kMinBlocks) sampler_kerne
         s.a_drained = 0;
         s.a_polls = 0;
         s.a_nap = 256;
+        s.a_spin = L.hdr->wait_polls;
+        s.a_leave = 0;
     }
     for (;;) {
         if (threadIdx.x == 0) {
-            int32_t pick = L.assist.entries != nullptr ? join_entry<BLOCK>(L, s, blockIdx.x) : -1;
-            if (pick < 0 && !s.a_drained) {
+            int32_t pick = L.assist.entries != nullptr && !s.a_leave
+                               ? join_entry<BLOCK>(L, s, blockIdx.x)
+                               : -1;
+            if (pick < 0 && !s.a_drained && !s.a_leave) {
                 const uint32_t w = atomicAdd(&L.hdr->work, 1u);
                 s.work = w;
                 if (w < total) {
@@ -1155,7 +1172,7 @@ __global__ void __launch_bounds__(BLOCK, Shape<BLOCK>::kMinBlocks) sampler_kerne
             if (pick == -1) {
                 // no sample left: wait for posted levels, or leave
                 s.a_drained = 1;
-                if (L.assist.entries == nullptr || ++s.a_polls > kAssistPolls ||
+                if (L.assist.entries == nullptr || s.a_leave || ++s.a_polls > kAssistPolls ||
                     ld_acquire_u32(&L.hdr->finished) >= total) {
                     pick = -2;
                 } else {
@@ -1251,6 +1268,19 @@ __global__ void __launch_bounds__(BLOCK, Shape<BLOCK>::kMinBlocks) sampler_kerne
         // ---- balanced bidirectional BFS (:89-144) ------------------------------
         uint32_t exp_side = kSideU;
         for (;;) {
+            // Levels that other samples posted on the board come before this
+            // sample's next level: a wide level ends sooner the more CTAs
+            // take its tiles, and the launch lasts as long as its slowest
+            // sample.  (Nothing of this sample's state is touched meanwhile.)
+            if (L.assist.entries != nullptr) {
+                for (;;) {
+                    if (threadIdx.x == 0) s.a_entry = join_entry<BLOCK>(L, s, blockIdx.x);
+                    __syncthreads();
+                    if (s.a_entry < 0) break;
+                    help_entry<BLOCK>(L, s, (uint32_t)s.a_entry);
+                    __syncthreads();
+                }
+            }
             const bool side_u = s.sum_u <= s.sum_v;
             exp_side = side_u ? kSideU : kSideV;
             const uint32_t lo = side_u ? s.start_u : s.start_v;
@@ -1495,6 +1525,7 @@ __global__ void __launch_bounds__(BLOCK, Shape<BLOCK>::kMinBlocks) sampler_kerne
             const unsigned long long dc = (unsigned long long)(clock64() - t_sample0);
             atomicAdd(&L.hdr->cycles, dc);
             atomicMax(&L.hdr->max_cycles, dc);
+            if (s.a_leave) atomicAdd(&L.hdr->failed, 1u);
             __threadfence();
             atomicAdd(&L.hdr->finished, 1u);
         }
@@ -1511,8 +1542,20 @@ __global__ void round_begin_kernel(SamplerLaunch L, uint32_t max_segs) {
         L.hdr->open_mask = 0;
         L.hdr->assisted = 0;
         L.hdr->helper_tiles = 0;
+        L.hdr->failed = 0;
         L.hdr->cycles = 0;
         L.hdr->max_cycles = 0;
+    }
+    // No sampler CTA runs between two launches: a board entry that a failed
+    // wait left closed (or any entry not free) is handed back here, with its
+    // generation advanced and nobody inside.
+    if (L.assist.entries != nullptr && threadIdx.x < kAssistEntries) {
+        AssistEntry *E = L.assist.entries + threadIdx.x;
+        const uint32_t st = E->state;
+        if ((st & 3u) != 0u) {
+            E->state = ((st >> 2) + 1u) << 2;
+            E->inside = 0u;
+        }
     }
 }
 

@@ -63,8 +63,18 @@ struct RoundHeader {
     uint32_t open_mask;     // help-board entries with tiles left (zeroed by round_begin)
     uint32_t assisted;      // levels expanded with help (zeroed by round_begin)
     uint32_t helper_tiles;  // tiles of those levels done by helpers (zeroed by round_begin)
+    // samples whose shared level gave up a wait (zeroed by round_begin); the
+    // CTA of such a sample leaves the launch, because helpers may still write
+    // to its slot, and the host re-initialises every slot after the launch
+    uint32_t failed;
+    uint32_t wait_polls;  // polls of each bounded help-board wait (set by the host)
     uint32_t pad;
 };
+
+// Polls of a bounded help-board wait unless the caller asks otherwise
+// (silvan_params_t::wait_polls): at >= 64 ns per poll well above any real
+// wait, which ends within microseconds.
+constexpr uint32_t kDefaultWaitPolls = 1u << 20;
 
 // Help board of a launch.  A CTA whose sample reaches a wide BFS level posts
 // it on a free entry; CTAs between two samples, and CTAs left without samples

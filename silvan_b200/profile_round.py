@@ -17,6 +17,12 @@ GRAPHS = {
     # name: (generator, job parameters)
     "rmat20": (lambda: sb.HostGraph.from_pairs(sb.rmat(20, 16, 2, True), True),
                dict(eps=0.005, delta=0.05)),
+    # the same generator at 2^18 and 2^17 nodes: every resident slot fits in
+    # a few GB, so a capture can run the sampler at full occupancy
+    "rmat18": (lambda: sb.HostGraph.from_pairs(sb.rmat(18, 16, 2, True), True),
+               dict(eps=0.005, delta=0.05)),
+    "rmat17": (lambda: sb.HostGraph.from_pairs(sb.rmat(17, 16, 2, True), True),
+               dict(eps=0.005, delta=0.05)),
     "grid2048": (lambda: sb.HostGraph.from_pairs(sb.grid(2048, 0.05, 0.001, 3), False),
                  dict(eps=0.1, delta=0.05, k=10, alpha=0.0, alpha_given=True)),
     "ba10k": (lambda: sb.HostGraph.from_pairs(sb.barabasi_albert(10000, 5, 1), False),

@@ -46,3 +46,30 @@ def test_reference_arm_other_ranks_exit_quietly():
                   env={"RANK": "1", "WORLD_SIZE": "2", "LOCAL_RANK": "1"})
     assert r.returncode == 0, r.stderr
     assert not [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+
+
+@pytest.mark.skipif(not os.path.exists(REF_LIB), reason="reference build not present")
+def test_reference_arm_loads_no_product_code():
+    """The reference arm generates its graph inside the reference harness
+    (oracle/_ref/libsilvan_refbench.so), so its process maps no library of
+    this project and imports no part of the package; the graph is the GPU
+    arm's graph (same CSR checksum)."""
+    code = (
+        "import sys, json, types; sys.argv = ['bench.py', '--impl', 'reference', '--config', "
+        "'ba10k', '--steps', '1', '--warmup', '0']; import bench; bench.main(); "
+        "maps = open('/proc/self/maps').read(); "
+        "print(json.dumps({'mods': [m for m in sys.modules if m.startswith('silvan_b200')], "
+        "'lib': 'libsilvan_b200' in maps, 'ref': 'libsilvan_refbench' in maps}))")
+    e = dict(os.environ)
+    for k in ("RANK", "WORLD_SIZE", "LOCAL_RANK"):
+        e.pop(k, None)
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=300,
+                       env=e, cwd=ROOT)
+    assert r.returncode == 0, r.stderr
+    lines = [json.loads(ln) for ln in r.stdout.splitlines() if ln.startswith("{")]
+    line, probe = lines[0], lines[-1]
+    assert probe == {"mods": [], "lib": False, "ref": True}
+    import bench
+    import silvan_b200 as sb
+    csr = bench.make_graph(bench.CONFIGS["ba10k"]).csr()
+    assert line["config"]["csr_sha1_16"] == bench.csr_checksum(csr)

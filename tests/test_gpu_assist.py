@@ -93,3 +93,34 @@ def test_replay_with_assisted_levels_matches_oracle(sb, port):
     np.testing.assert_array_equal(got["offsets"], want.offsets)
     np.testing.assert_array_equal(got["nodes"], want.nodes)
     np.testing.assert_array_equal(got["counts"], want.counts)
+
+
+def test_failed_shared_level_does_not_leak_into_later_jobs(sb, port, small_graphs):
+    """Failure path of the help board.  With no polls allowed, every wait
+    between the CTAs of a shared level gives up at once: the owner's level is
+    marked failed while helpers may still be inside it, so records of its
+    slot can be left half-written.  The job must fail with E_TIMEOUT, and the
+    next jobs, which borrow the same pooled sampler engine (its slots and its
+    board), must again match the oracle bit for bit with the board in use:
+    the engine re-initialises the slots after such a launch and reopens the
+    board entries that stayed closed.  The reference's own per-sample reset
+    (silvan/src/Sp_sampler.cpp:226-231) is what these jobs rely on."""
+    hg, csr, _ = small_graphs["rmat11d"]
+    g = sb.Graph.from_host(hg)
+    bad = sb.Probabilistic(g, 0.03, 0.1, seed=5, block=128, assist_items=1, wait_polls=NEVER)
+    with pytest.raises(sb.SilvanError) as err:
+        bad.run()
+    assert err.value.code == sb.E_TIMEOUT
+    del bad
+    for seed, items in ((5, 1), (6, 0)):
+        job = sb.Probabilistic(g, 0.03, 0.1, seed=seed, block=128, assist_items=items)
+        res = job.run()
+        if items == 1:
+            assert res["assisted_levels"] > 0
+        o = port_graph(port, csr).run(csr.diameter, 0.03, 0.1, seed=seed)
+        for f in ("num_samples", "vis_edges", "iteration_index", "first_pass_samples",
+                  "stop_reason"):
+            assert res[f] == o[f], (seed, f, res[f], o[f])
+        c = job.counters()
+        for f in ("approx", "wimpy", "mcrade"):
+            np.testing.assert_array_equal(c[f], o[f], err_msg=f"seed {seed}: {f}")

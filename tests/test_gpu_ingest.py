@@ -112,3 +112,24 @@ def test_undirected_components_on_the_device(sb, tmp_path, make):
     host = sb.HostGraph.load(path, False).csr()
     assert host.n_components > 10
     assert_same_graph(dev, host)
+
+
+@pytest.mark.parametrize("make", [
+    lambda sb: sb.rmat(14, 4, 9, True),            # thousands of components, shallow
+    lambda sb: sb.rmat(12, 2, 3, True),            # sparse: many singleton components
+    # a chain of 300 components with a few short cycles: deeper than the
+    # device's passes, so the recursion ends on the host copy
+    lambda sb: np.array([[i, i + 1] for i in range(300)] + [[5, 2], [100, 90], [250, 249]],
+                        np.uint32),
+])
+def test_directed_bound_on_the_device(sb, tmp_path, make):
+    """Directed graphs: the component numbers are the host's Tarjan order,
+    and the diameter bound over them (pivots, eccentricities inside each
+    component, the AllCCUpperBound recursion) is computed on the device; it
+    must equal the host's restatement of the reference."""
+    path = str(tmp_path / "d.txt")
+    sb.write_edge_list(path, make(sb))
+    dev = sb.Graph.load(path, True).csr()
+    host = sb.HostGraph.load(path, True).csr()
+    assert host.n_components > 10
+    assert_same_graph(dev, host)
