@@ -62,9 +62,10 @@ CONFIGS = {
     "multigraph64": dict(kind="multi", workload="64_graphs_er8_ba4_n1e3_2e6_seeds100_163",
                          eps=0.01, delta=0.05),
     # Poisson request stream of fresh R-MAT graphs (scale 10-20, directed
-    # with probability 1/2, eps in {0.01, 0.005, 0.0025}, top-10 on 20 %; the
-    # top-10 requests take their relative eps as 10 x that draw: at relative
-    # eps 0.01 one scale-20 top-10 request alone needs over 4 * 10^7 samples)
+    # with probability 1/2, eps in {0.01, 0.005, 0.0025}, top-10 on 20 %);
+    # --topk-eps-scale multiplies the top-10 requests' relative eps (at
+    # relative eps 0.01 one scale-20 top-10 request alone needs over 4 * 10^7
+    # samples)
     "serve": dict(kind="serve", workload="rmat_scale10_20_poisson_stream", delta=0.05),
     # Graph(filename) on the R-MAT 20 edge list: device parse + CSR build
     # (silvan_graph_load) against the host loader and the reference's own
@@ -563,7 +564,7 @@ def run_serve(args, cfg):
         eps = float(rng.choice([0.01, 0.005, 0.0025]))
         k = 10 if rng.random() < 0.2 else 0
         if k:
-            eps *= 10.0
+            eps *= args.topk_eps_scale
         reqs.append((scale, d, eps, k, float(rng.exponential(1.0 / args.rate))))
     srv = sb.Server(1 << 20, slots=args.slots)
     try:
@@ -610,6 +611,8 @@ def run_serve(args, cfg):
         "dtype": "u32/u64/f64", "data": "synthetic",
         "config": {"workload": cfg["workload"], "requests": len(reqs),
                    "rate_per_s": args.rate, "delta": cfg["delta"],
+                   "topk_eps": ("the drawn eps, as the workload states" if args.topk_eps_scale == 1
+                                else f"{args.topk_eps_scale:g} x the drawn eps"),
                    "graphs": "22 pre-generated R-MAT graphs (scale 10-20 x directed or not), "
                              "each request uploads and estimates its own copy",
                    "latency": "host clock from submission to the finished result"},
@@ -730,6 +733,9 @@ def main():
     ap.add_argument("--rate", type=float, default=4.0, help="serve: Poisson arrivals per second")
     ap.add_argument("--slo-ms", type=float, default=2500.0,
                     help="serve: stated p99 objective over all requests")
+    ap.add_argument("--topk-eps-scale", type=float, default=1.0,
+                    help="serve: top-10 requests use this multiple of the drawn eps as their "
+                         "relative eps (1 = the workload as stated)")
     args = ap.parse_args()
     cfg = CONFIGS[args.config]
     if args.impl == "reference":

@@ -336,7 +336,9 @@ int silvan_replay_samples(silvan_graph_t g, uint64_t seed, uint32_t first, uint3
  * unordered, whose sample field is the index relative to `first` (0 for
  * sample `first`), and *d_record_count their number (when it exceeds
  * record_cap the surplus is dropped and the affected samples carry
- * SILVAN_E_CAPACITY).  The work is queued on `stream` (a cudaStream_t, NULL
+ * SILVAN_E_CAPACITY; slots below record_cap that such a sample had reserved
+ * hold placeholders with count 0 and node 0xFFFFFFFF, to be skipped).  The
+ * work is queued on `stream` (a cudaStream_t, NULL
  * for the default stream); outputs are ready when the stream reaches it.  The
  * first call on a device looks up the scratch's device address (and caches
  * it: the cache does not survive cudaDeviceReset), so it should come before

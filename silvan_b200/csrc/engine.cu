@@ -1,6 +1,7 @@
 // Host engine (see engine.h).
 #include "engine.h"
 #include "components.h"
+#include "graph_dev.cuh"
 
 #include <algorithm>
 #include <atomic>
@@ -264,6 +265,19 @@ int DeviceGraph::upload() {
     }
     RK(dmalloc(&d_cc, n));
     CK(cudaMemcpy(d_cc, cc.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice));
+    return make_rows(cudaStreamLegacy);
+}
+
+int DeviceGraph::make_rows(cudaStream_t stream) {
+    RK(dmalloc(&d_out_rows, n));
+    CK(silvan::make_rows(d_out_off, d_out_rows, n, stream));
+    if (d_in_off != d_out_off) {
+        RK(dmalloc(&d_in_rows, n));
+        CK(silvan::make_rows(d_in_off, d_in_rows, n, stream));
+    } else {
+        d_in_rows = d_out_rows;
+    }
+    CK(cudaStreamSynchronize(stream));
     return SILVAN_OK;
 }
 
@@ -352,16 +366,19 @@ int DeviceGraph::upload_raw(uint32_t nn, bool dir, const uint64_t *out_off,
         set_error("CSR rows must hold ascending unique ids < n");
         return SILVAN_E_BADARG;
     }
-    return SILVAN_OK;
+    return make_rows(cudaStreamLegacy);
 }
 
 uint64_t DeviceGraph::device_bytes() const {
-    uint64_t b = 4ull * (n + 1) + 4ull * m + 4ull * n;
-    if (directed) b += 4ull * (n + 1) + 4ull * m_in;
+    uint64_t b = 4ull * (n + 1) + 4ull * m + 4ull * n + 8ull * n;
+    if (directed) b += 4ull * (n + 1) + 4ull * m_in + 8ull * n;
     return b;
 }
 
 DeviceGraph::~DeviceGraph() {
+    if (d_in_rows != d_out_rows) dfree(d_in_rows);
+    d_in_rows = nullptr;
+    dfree(d_out_rows);
     if (d_in_off != d_out_off) dfree(d_in_off);
     if (d_in_adj != d_out_adj) dfree(d_in_adj);
     d_in_off = d_in_adj = nullptr;
@@ -629,6 +646,8 @@ int Engine::round(const std::vector<Job *> &jobs, const std::vector<JobRequest> 
         RoundBuffers &rb = job->round_buffers();
         SegDesc &S = h_segs_[s];
         S.out_off = G.d_out_off;
+        S.out_rows = G.d_out_rows;
+        S.in_rows = G.d_in_rows;
         S.out_adj = G.d_out_adj;
         S.in_off = G.d_in_off;
         S.in_adj = G.d_in_adj;
@@ -768,6 +787,18 @@ int Engine::round(const std::vector<Job *> &jobs, const std::vector<JobRequest> 
     }
     for (uint32_t s = 0; s < idx.size(); s++) records[idx[s]] = h_cursors_[s];
     return SILVAN_OK;
+}
+
+uint64_t Engine::job_hint(const DeviceGraph *G) const {
+    auto it = job_total_.find(G->tune_class());
+    return it == job_total_.end() ? 0 : it->second;
+}
+
+void Engine::note_job(const DeviceGraph *G, uint64_t used, bool alpha_kept) {
+    // only a job whose second pass kept the first pass's alpha can use
+    // samples drawn ahead in its first launch
+    if (alpha_kept) job_total_[G->tune_class()] = used;
+    else job_total_.erase(G->tune_class());
 }
 
 uint32_t Engine::free_samples(const DeviceGraph *G, bool tail_only) const {
@@ -1502,6 +1533,12 @@ bool Job::next_request(JobRequest &r) {
         // would otherwise ask for a launch whose size favours long tails
         uint64_t ahead = phase_ == kPass2 ? lookahead_
                                           : std::min<uint64_t>(lookahead_tail_, 4 * target_);
+        if (phase_ == kPass1 && hint_total_ > target_) {
+            // the last job of this class of graphs used hint_total_ samples
+            // with pass 2 on the same stream: draw that far at once (10 %
+            // more), so that one launch usually covers the whole estimation
+            ahead = std::max<uint64_t>(ahead, hint_total_ + hint_total_ / 10 - target_);
+        }
         if (phase_ == kPass2 && predicted_stop_ > pass_samples_) {
             // absolute mode after a failed check: up to the schedule point at
             // or after the predicted stop (at most 4x the samples so far)
@@ -1873,6 +1910,7 @@ int Job::run(silvan_result_t *res, FILE *sink) {
     std::vector<JobRequest> reqs(1);
     std::vector<uint64_t> nrec;
     set_lookahead(own_engine_->free_samples(g_, true), own_engine_->free_samples(g_, false));
+    hint_total_ = own_engine_->job_hint(g_);
     while (!done()) {
         if (!next_request(reqs[0])) {
             set_error("sample index space exhausted");
@@ -1886,7 +1924,12 @@ int Job::run(silvan_result_t *res, FILE *sink) {
         }
         set_lookahead(own_engine_->free_samples(g_, true), own_engine_->free_samples(g_, false));
     }
-    return finish(res);
+    RK(finish(res));
+    // the next job of this class of graphs draws about as far in its first
+    // launch (when the second pass kept alpha, so those draws are used)
+    own_engine_->note_job(g_, result_.first_pass_samples + result_.num_samples,
+                          alpha_ == p_.alpha);
+    return SILVAN_OK;
 }
 
 int Job::step(uint32_t rounds, silvan_status_t *st, FILE *sink) {

@@ -57,6 +57,9 @@ struct DeviceGraph {
     uint32_t *d_out_off = nullptr, *d_out_adj = nullptr;
     uint32_t *d_in_off = nullptr, *d_in_adj = nullptr;
     uint32_t *d_cc = nullptr;
+    // (start, end) of every row, for the sampler: in_rows aliases out_rows
+    // for undirected graphs
+    uint2 *d_out_rows = nullptr, *d_in_rows = nullptr;
     int device = 0;
     // Class of the graph for the sampler's schedule statistics: graphs with
     // the same direction, node count and mean degree (both to a power of 2)
@@ -69,6 +72,9 @@ struct DeviceGraph {
     int upload_raw(uint32_t n, bool directed, const uint64_t *out_off, const uint32_t *out_adj,
                    const uint64_t *in_off, const uint32_t *in_adj, const uint32_t *cc);
     uint64_t device_bytes() const;
+    // d_out_rows / d_in_rows from the device offsets (every upload path ends
+    // with it)
+    int make_rows(cudaStream_t stream);
     // Components and diameter bound on the host copy, then the component
     // ids to the device (after a device ingest filled d_* and `host`).
     int finish_from_host_copy();
@@ -126,6 +132,10 @@ class Engine {
     // drawing (0 until a launch has been measured)
     // measured on the last launch that drew samples of G's class of graphs
     uint32_t free_samples(const DeviceGraph *G, bool tail_only) const;
+    // Samples (both passes) the last single-job run on G's class of graphs
+    // used, when its second pass kept alpha (0: none recorded)
+    uint64_t job_hint(const DeviceGraph *G) const;
+    void note_job(const DeviceGraph *G, uint64_t used, bool alpha_kept);
     uint64_t launches() const { return launches_; }
     float sample_ms() const { return sample_ms_; }
     void reset_timers() {
@@ -197,6 +207,7 @@ class Engine {
         uint32_t samples = 0;  // drawn by the launch
     };
     std::unordered_map<uint64_t, LastLaunch> last_;  // by tune_class()
+    std::unordered_map<uint64_t, uint64_t> job_total_;  // by tune_class(): see job_hint
 };
 
 class Job {
@@ -303,6 +314,7 @@ class Job {
     uint64_t base_global_ = 0;   // global index of the pass's first sample
     uint32_t lookahead_ = 0;     // pass 2: samples drawn ahead of the next point
     uint32_t lookahead_tail_ = 0;  // pass 1 (absolute mode): samples drawn beyond it
+    uint64_t hint_total_ = 0;      // samples the last job of this graph class used
     uint64_t predicted_stop_ = 0;  // pass 2 (absolute mode): sample size of the likely stop
     float commit_ms_ = 0;
     uint64_t drawn_ = 0;         // samples drawn over both passes

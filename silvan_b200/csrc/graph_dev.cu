@@ -27,7 +27,17 @@ __global__ void validate_rows_kernel(const uint32_t *off, const uint32_t *adj, u
     }
 }
 
+__global__ void make_rows_kernel(const uint32_t *off, uint2 *rows, uint32_t n) {
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x)
+        rows[v] = make_uint2(off[v], off[v + 1]);
+}
+
 }  // namespace
+
+cudaError_t make_rows(const uint32_t *off, uint2 *rows, uint32_t n, cudaStream_t s) {
+    make_rows_kernel<<<592, 256, 0, s>>>(off, rows, n);
+    return cudaGetLastError();
+}
 
 cudaError_t narrow_offsets(const uint64_t *in, uint32_t *out, uint32_t count, cudaStream_t s) {
     narrow_offsets_kernel<<<592, 256, 0, s>>>(in, out, count);

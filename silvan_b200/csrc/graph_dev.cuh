@@ -8,6 +8,9 @@
 namespace silvan {
 
 cudaError_t narrow_offsets(const uint64_t *in, uint32_t *out, uint32_t count, cudaStream_t s);
+// rows[v] = (off[v], off[v + 1]) for v < n: a row's bounds in one 8-byte load
+// (one memory transaction where two 4-byte loads take two).
+cudaError_t make_rows(const uint32_t *off, uint2 *rows, uint32_t n, cudaStream_t s);
 // *bad (device) becomes nonzero when a row is not ascending and unique, when
 // an id is >= n, or when the offsets decrease.
 cudaError_t validate_rows(const uint32_t *off, const uint32_t *adj, uint32_t n, uint32_t *bad,

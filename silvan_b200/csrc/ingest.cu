@@ -387,6 +387,7 @@ int device_ingest(const char *path, bool directed, DeviceGraph &G, std::string &
     G.m = m;
     G.m_in = m_in;
     CKI(cudaGetDevice(&G.device));
+    RKI(G.make_rows(st));
     if (directed) {
         G.has_host = true;
         return G.finish_from_host_copy();

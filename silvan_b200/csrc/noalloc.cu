@@ -162,6 +162,8 @@ int replay_samples_noalloc(const DeviceGraph &G, uint64_t seed, uint32_t first, 
     }
     SegDesc sd{};
     sd.out_off = G.d_out_off;
+    sd.out_rows = G.d_out_rows;
+    sd.in_rows = G.d_in_rows;
     sd.out_adj = G.d_out_adj;
     sd.in_off = G.d_in_off;
     sd.in_adj = G.d_in_adj;

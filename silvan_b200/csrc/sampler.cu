@@ -39,6 +39,11 @@ namespace silvan {
 namespace {
 
 constexpr int kItems = 4;        // scan items per lane per tile
+// Samples a CTA takes from the round at once while many are left; one
+// thread each draws the endpoints and runs the void test, so the void
+// samples (most of them on sparse directed graphs) cost a fraction of a
+// sample each.  Near the end of a round the CTAs take one at a time.
+constexpr uint32_t kScreen = 8;
 constexpr int kMaxLevels = 256;  // levels per side with recorded bounds
 
 // Per-CTA-size constants: BLOCK threads serve one sample.  Smaller CTAs put
@@ -93,6 +98,10 @@ struct SamplerSmem {
     uint32_t a_drained, a_polls, a_nap;  // no sample left; board polls since; next nap (ns)
     uint32_t a_spin;    // polls of a bounded wait (RoundHeader::wait_polls)
     uint32_t a_leave;   // a shared level of this CTA's sample failed: take no more samples
+    // samples taken from the round in a chunk and screened in parallel: the
+    // void ones are finished at once, the others wait here
+    uint32_t pend_w[kScreen];
+    uint32_t pend_n, pend_i, scr_w0, scr_v;
 };
 
 __device__ __forceinline__ uint32_t lanemask_lt() {
@@ -142,10 +151,22 @@ __device__ uint32_t block_exclusive_scan(uint32_t v, uint32_t &excl, uint32_t *t
     return total;
 }
 
+// The neutral record (st, cnt, sigma = 0; first = ~0; last = 0) in one
+// 32-byte store: a node record is one sector, written by one transaction.
 __device__ __forceinline__ void rec_reset(NodeRec *r) {
-    uint4 *p = reinterpret_cast<uint4 *>(r);
-    p[0] = make_uint4(0u, 0u, 0u, 0u);                  // st, cnt, sigma
-    p[1] = make_uint4(0xffffffffu, 0xffffffffu, 0u, 0u);  // first = ~0, last = 0
+    asm volatile("st.global.v8.b32 [%0], {%1, %1, %1, %1, %2, %2, %1, %1};" ::"l"(r), "r"(0u),
+                 "r"(0xffffffffu)
+                 : "memory");
+}
+
+// A whole record in one 32-byte load through L2 (the slot is written by this
+// CTA and, for shared levels, by others): words 0-3 and 4-7.
+__device__ __forceinline__ void rec_load(const NodeRec *r, uint4 &lo, uint4 &hi) {
+    asm volatile("ld.global.cg.v8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                 : "=r"(lo.x), "=r"(lo.y), "=r"(lo.z), "=r"(lo.w), "=r"(hi.x), "=r"(hi.y),
+                   "=r"(hi.z), "=r"(hi.w)
+                 : "l"(r)
+                 : "memory");
 }
 
 // Predecessor of rank t (queue order) of node a, 0 < t < cnt - 1.  The
@@ -162,24 +183,26 @@ __device__ uint32_t middle_pred(const SegDesc &A, const Smem &s, const NodeRec *
     const uint32_t side = st_side(st_a);
     const uint32_t dprev = st_dist(st_a) - 1u;
     const uint32_t want = st_make(side, dprev);
-    const uint32_t *roff = side == kSideU ? A.in_off : A.out_off;
+    const uint2 *rrows = side == kSideU ? A.in_rows : A.out_rows;
     const uint32_t *radj = side == kSideU ? A.in_adj : A.out_adj;
-    const uint32_t *foff = side == kSideU ? A.out_off : A.in_off;
+    const uint2 *frows = side == kSideU ? A.out_rows : A.in_rows;
     const uint32_t *fadj = side == kSideU ? A.out_adj : A.in_adj;
-    const uint32_t rb = roff[a], re = roff[a + 1];
+    const uint2 rr = rrows[a];
+    const uint32_t rb = rr.x, re = rr.y;
     if (dprev < (uint32_t)kMaxLevels) {
         const uint32_t lo = s.lvl_lo[side - 1][dprev], hi = s.lvl_hi[side - 1][dprev];
         if ((uint64_t)(hi - lo) * 24u < (uint64_t)(re - rb)) {
             uint32_t seen = 0;
             for (uint32_t i = lo; i < hi; i++) {
                 const uint32_t x = __ldcg(&queue[i]);
-                uint32_t l = foff[x], h = foff[x + 1];
+                const uint2 fr = frows[x];
+                uint32_t l = fr.x, h = fr.y;
                 while (l < h) {  // first entry >= a
                     const uint32_t mid = (l + h) >> 1;
                     if (fadj[mid] < a) l = mid + 1;
                     else h = mid;
                 }
-                if (l < foff[x + 1] && fadj[l] == a) {
+                if (l < fr.y && fadj[l] == a) {
                     if (seen == t) return x;
                     seen++;
                 }
@@ -241,9 +264,9 @@ __device__ uint32_t weighted_pred(const SegDesc &A, const NodeRec *rec, uint32_t
                                   uint32_t st_a, uint32_t cnt, uint32_t r, int32_t &status) {
     const uint32_t side = st_side(st_a);
     const uint32_t want = st_make(side, st_dist(st_a) - 1u);
-    const uint32_t *roff = side == kSideU ? A.in_off : A.out_off;
+    const uint2 rr = (side == kSideU ? A.in_rows : A.out_rows)[a];
     const uint32_t *radj = side == kSideU ? A.in_adj : A.out_adj;
-    const uint32_t rb = roff[a], re = roff[a + 1];
+    const uint32_t rb = rr.x, re = rr.y;
     unsigned long long acc = 0, prev = 0;
     bool have_prev = false;
     uint32_t last = a;
@@ -289,7 +312,7 @@ __device__ void expand_level(const SegDesc &A, SamplerSmem<BLOCK> &s, NodeRec *r
     constexpr int kTile = Shape<BLOCK>::kTile;
     constexpr int kChunk = Shape<BLOCK>::kChunk;
     constexpr int kPer = Shape<BLOCK>::kPerThread;
-    const uint32_t *off = side == kSideU ? A.out_off : A.in_off;
+    const uint2 *rows = side == kSideU ? A.out_rows : A.in_rows;
     const uint32_t *adj = side == kSideU ? A.out_adj : A.in_adj;
     const uint32_t new_st = st_make(side, depth + 1u);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -312,8 +335,9 @@ __device__ void expand_level(const SegDesc &A, SamplerSmem<BLOCK> &s, NodeRec *r
             o0[i] = o1[i] = 0;
             sg[i] = 0;
             if (p < nc) {
-                o0[i] = __ldg(&off[xq[i]]);
-                o1[i] = __ldg(&off[xq[i] + 1]);
+                const uint2 r = __ldg(&rows[xq[i]]);
+                o0[i] = r.x;
+                o1[i] = r.y;
                 sg[i] = __ldcg(&rec[xq[i]].sigma);
             }
         }
@@ -370,7 +394,8 @@ __device__ void expand_level(const SegDesc &A, SamplerSmem<BLOCK> &s, NodeRec *r
 #pragma unroll
             for (int k = 0; k < kItems; k++) {
                 sty[k] = code[k] ? __ldcg(&rec[ys[k]].st) : 0u;
-                dg[k] = code[k] ? __ldg(&off[ys[k] + 1]) - __ldg(&off[ys[k]]) : 0u;
+                const uint2 r = code[k] ? __ldg(&rows[ys[k]]) : make_uint2(0u, 0u);
+                dg[k] = r.y - r.x;
             }
 #pragma unroll
             for (int k = 0; k < kItems; k++) {
@@ -705,9 +730,10 @@ __device__ __forceinline__ int32_t post_level(const SamplerLaunch &L, SamplerSme
                                            bool side_u, uint32_t lo, uint32_t hi,
                                            uint32_t depth) {
     const SegDesc &A = s.seg;
-    const uint32_t *doff = side_u ? A.out_off : A.in_off;
+    const uint2 *drows = side_u ? A.out_rows : A.in_rows;
     const uint32_t x0 = side_u ? s.u : s.v;
-    const uint32_t items = depth == 0 ? doff[x0 + 1] - doff[x0] : (side_u ? s.sum_u : s.sum_v);
+    const uint2 r0 = drows[x0];
+    const uint32_t items = depth == 0 ? r0.y - r0.x : (side_u ? s.sum_u : s.sum_v);
     const uint32_t F = hi - lo;
     const uint32_t thr =
         A.assist_items == kAssistItemsAuto ? 8u * (uint32_t)Shape<BLOCK>::kTile : A.assist_items;
@@ -832,7 +858,8 @@ __device__ void assist_tile(SamplerSmem<BLOCK> &s, const AssistBoard &B, uint32_
         fv[k] = code[k] == 1
                     ? __ldcg(reinterpret_cast<const unsigned long long *>(&V.rec[ys[k]].first))
                     : 0ull;
-        dg[k] = code[k] == 1 ? __ldg(&V.off[ys[k] + 1]) - __ldg(&V.off[ys[k]]) : 0u;
+        const uint2 r = code[k] == 1 ? __ldg(&V.rows[ys[k]]) : make_uint2(0u, 0u);
+        dg[k] = r.y - r.x;
     }
     uint32_t rnm[kItems];  // rank among the warp's joins (low half) and meeting edges
 #pragma unroll
@@ -968,7 +995,7 @@ __device__ bool expand_level_assisted(const SamplerLaunch &L, const SegDesc &A,
     constexpr int kPer = Shape<BLOCK>::kPerThread;
     const AssistBoard &B = L.assist;
     AssistEntry *E = B.entries + e;
-    const uint32_t *off = side == kSideU ? A.out_off : A.in_off;
+    const uint2 *rows = side == kSideU ? A.out_rows : A.in_rows;
     const uint32_t *adj = side == kSideU ? A.out_adj : A.in_adj;
     const uint32_t F = hi - lo;
     const uint64_t tb = (uint64_t)e * B.tile_cap;
@@ -992,8 +1019,9 @@ __device__ bool expand_level_assisted(const SamplerLaunch &L, const SegDesc &A,
             const uint32_t p = threadIdx.x * kPer + i;
             o0[i] = o1[i] = 0u;
             if (p < nc) {
-                o0[i] = __ldg(&off[xq[i]]);
-                o1[i] = __ldg(&off[xq[i] + 1]);
+                const uint2 r = __ldg(&rows[xq[i]]);
+                o0[i] = r.x;
+                o1[i] = r.y;
             }
             tsum += o1[i] - o0[i];
         }
@@ -1053,7 +1081,7 @@ __device__ bool expand_level_assisted(const SamplerLaunch &L, const SegDesc &A,
             V.side = side;
             V.qbase = s.end_q;
             V.mbase = s.nmeet;
-            V.off = off;
+            V.rows = rows;
             V.adj = adj;
             V.rec = rec;
             V.queue = queue;
@@ -1121,6 +1149,69 @@ __device__ void help_entry(const SamplerLaunch &L, SamplerSmem<BLOCK> &s, uint32
     }
 }
 
+// Segment owning work index w: the last segment whose base is <= w.
+__device__ __forceinline__ uint32_t segment_of(const SegDesc *segs, uint32_t nsegs, uint32_t w) {
+    uint32_t l = 0, h = nsegs;
+    while (h - l > 1) {
+        const uint32_t mid = (l + h) >> 1;
+        if (segs[mid].base <= w) l = mid;
+        else h = mid;
+    }
+    return l;
+}
+
+// Takes the next kScreen work indices of the round (one while few are left)
+// and screens them, one thread each: endpoints (Sp_sampler.cpp:46,58-60)
+// and the void test (:62-74).  A void sample's outputs are written here; the
+// others are queued in s.pend_w for the full sampler.  Sets s.a_drained when
+// the round has no sample left.
+template <int BLOCK>
+__device__ __noinline__ void screen_chunk(const SamplerLaunch &L, SamplerSmem<BLOCK> &s,
+                                          uint32_t total, uint32_t nsegs) {
+    if (threadIdx.x == 0) {
+        const uint32_t taken = ld_acquire_u32(&L.hdr->work);
+        const uint32_t left = taken < total ? total - taken : 0u;
+        const uint32_t v = left > 2u * kScreen * gridDim.x ? kScreen : 1u;
+        const uint32_t w0 = atomicAdd(&L.hdr->work, v);
+        s.scr_w0 = w0;
+        s.scr_v = v;
+        s.pend_n = 0;
+        s.pend_i = 0;
+        if (w0 >= total) s.a_drained = 1;
+    }
+    __syncthreads();
+    const uint32_t w = s.scr_w0 + threadIdx.x;
+    bool is_void = false;
+    if (threadIdx.x < s.scr_v && w < total) {
+        const long long t0 = clock64();
+        const SegDesc &A = L.segs[segment_of(L.segs, nsegs, w)];
+        const uint32_t gidx = A.first_sample + (w - A.base);
+        uint32_t d = 0;
+        uint32_t v = draw32(A.seed, gidx, d++) % A.n;
+        const uint32_t u = draw32(A.seed, gidx, d++) % A.n;
+        while (u == v) v = draw32(A.seed, gidx, d++) % A.n;
+        is_void = A.directed ? (A.cc[u] < A.cc[v]) : (A.cc[u] != A.cc[v]);
+        if (is_void) {
+            const uint32_t sl = w - A.base;
+            A.out_pl[sl] = 0;
+            A.out_np[sl] = 0;
+            A.out_vis[sl] = 0;
+            A.out_status[sl] = 0;
+            A.out_ball[sl] = 0;
+            A.out_pred[sl] = 0;
+            atomicAdd(&L.hdr->cycles, (unsigned long long)(clock64() - t0));
+        } else {
+            s.pend_w[atomicAdd(&s.pend_n, 1u)] = w;
+        }
+    }
+    const uint32_t nv = __syncthreads_count(is_void);
+    if (threadIdx.x == 0 && nv) {
+        __threadfence();
+        atomicAdd(&L.hdr->finished, nv);
+    }
+    __syncthreads();
+}
+
 template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK, Shape<BLOCK>::kMinBlocks) sampler_kernel(SamplerLaunch L) {
     constexpr int kWarps = Shape<BLOCK>::kWarps;
@@ -1149,24 +1240,35 @@ __global__ void __launch_bounds__(BLOCK, Shape<BLOCK>::kMinBlocks) sampler_kerne
         s.a_spin = L.hdr->wait_polls;
         s.a_leave = 0;
     }
+    if (threadIdx.x == 0) s.pend_n = s.pend_i = 0;
     for (;;) {
         if (threadIdx.x == 0) {
             int32_t pick = L.assist.entries != nullptr && !s.a_leave
                                ? join_entry<BLOCK>(L, s, blockIdx.x)
                                : -1;
-            if (pick < 0 && !s.a_drained && !s.a_leave) {
-                const uint32_t w = atomicAdd(&L.hdr->work, 1u);
+            if (pick < 0 && !s.a_leave && s.pend_i < s.pend_n) {
+                const uint32_t w = s.pend_w[s.pend_i++];
                 s.work = w;
-                if (w < total) {
-                    // segment owning work index w: last segment with base <= w
-                    uint32_t l = 0, h = nsegs;
-                    while (h - l > 1) {
-                        const uint32_t mid = (l + h) >> 1;
-                        if (L.segs[mid].base <= w) l = mid;
-                        else h = mid;
-                    }
-                    s.sample = l;
-                    pick = -3;  // a sample
+                s.sample = segment_of(L.segs, nsegs, w);
+                pick = -3;  // a sample
+            } else if (pick < 0 && !s.a_drained && !s.a_leave) {
+                pick = -4;  // take the next chunk of the round
+            }
+            if (pick == -1 && s.a_leave) {
+                // this CTA leaves the launch (its slot may be inconsistent):
+                // the samples it screened but has not run are reported failed
+                for (; s.pend_i < s.pend_n; s.pend_i++) {
+                    const uint32_t w = s.pend_w[s.pend_i];
+                    const SegDesc &B = L.segs[segment_of(L.segs, nsegs, w)];
+                    const uint32_t sl = w - B.base;
+                    B.out_pl[sl] = 0;
+                    B.out_np[sl] = 0;
+                    B.out_vis[sl] = 0;
+                    B.out_status[sl] = SILVAN_E_TIMEOUT;
+                    B.out_ball[sl] = 0;
+                    B.out_pred[sl] = 0;
+                    __threadfence();
+                    atomicAdd(&L.hdr->finished, 1u);
                 }
             }
             if (pick == -1) {
@@ -1194,6 +1296,10 @@ __global__ void __launch_bounds__(BLOCK, Shape<BLOCK>::kMinBlocks) sampler_kerne
         if (pick == -2) break;
         if (pick == -1) {
             __syncthreads();
+            continue;
+        }
+        if (pick == -4) {
+            screen_chunk<BLOCK>(L, s, total, nsegs);
             continue;
         }
         {
@@ -1412,8 +1518,8 @@ __global__ void __launch_bounds__(BLOCK, Shape<BLOCK>::kMinBlocks) sampler_kerne
                                 break;
                             }
                             // the whole record (one sector) in one load
-                            const uint4 r0 = __ldcg(reinterpret_cast<const uint4 *>(&rec[a]));
-                            const uint4 r1 = __ldcg(reinterpret_cast<const uint4 *>(&rec[a]) + 1);
+                            uint4 r0, r1;
+                            rec_load(&rec[a], r0, r1);
                             if (pend != 0xffffffffu && pend_old == 0u) {
                                 const uint32_t ti = atomicAdd(&s.ntouched, 1u);
                                 touched[ti] = pend;
@@ -1470,7 +1576,7 @@ __global__ void __launch_bounds__(BLOCK, Shape<BLOCK>::kMinBlocks) sampler_kerne
         // ---- emit the path map, restore the slot ---------------------------------
         const uint32_t nt = s.ntouched;
         if (threadIdx.x == 0) {
-            unsigned long long b = 0;
+            unsigned long long b = ~0ull;
             if (nt > 0 && s.status == 0) {
                 b = atomicAdd(A.rec_cursor, (unsigned long long)nt);
                 if (b + nt > A.rec_cap) s.status = SILVAN_E_CAPACITY;
@@ -1480,6 +1586,10 @@ __global__ void __launch_bounds__(BLOCK, Shape<BLOCK>::kMinBlocks) sampler_kerne
         __syncthreads();
         const unsigned long long rb = s.rec_base;
         const bool emit = s.status == 0;
+        // A sample whose path map did not fit may have reserved slots below
+        // the buffer's end: they get placeholders (count 0, node ~0) of this
+        // sample, so that every slot below the end holds a defined record.
+        const bool fill = !emit && rb < A.rec_cap;
         for (uint32_t i0 = threadIdx.x; i0 < nt; i0 += 4 * BLOCK) {
             uint32_t a4[4], c4[4];
 #pragma unroll
@@ -1498,6 +1608,12 @@ __global__ void __launch_bounds__(BLOCK, Shape<BLOCK>::kMinBlocks) sampler_kerne
                     pr.node = a4[j];
                     pr.sample = sl;
                     pr.count = c4[j];
+                    A.recs[rb + i] = pr;
+                } else if (fill && rb + i < A.rec_cap) {
+                    PathRec pr;
+                    pr.node = 0xffffffffu;
+                    pr.sample = sl;
+                    pr.count = 0;
                     A.recs[rb + i] = pr;
                 }
                 hits[a4[j]] = 0;

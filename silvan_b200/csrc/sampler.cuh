@@ -24,6 +24,8 @@ struct SegDesc {
     const uint32_t *in_off;   // alias out_* when undirected
     const uint32_t *in_adj;
     const uint32_t *cc;
+    const uint2 *out_rows;  // (start, end) of each row; alias when undirected
+    const uint2 *in_rows;
     uint32_t n;
     int32_t directed;
     uint64_t seed;
@@ -87,7 +89,7 @@ constexpr uint32_t kAssistEntries = 8;
 struct AssistLevel {
     uint32_t ntiles, items, nodes, lo;
     uint32_t new_st, side, qbase, mbase;
-    const uint32_t *off;  // rows in the expansion direction
+    const uint2 *rows;    // (start, end) of the rows in the expansion direction
     const uint32_t *adj;
     NodeRec *rec;         // the owner's slot
     uint32_t *queue;

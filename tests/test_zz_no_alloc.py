@@ -38,6 +38,8 @@ def noalloc_replay(sb, g, seed, first, count, alpha, cap, allow_overflow=False):
     n_rec = int(cnt.item())
     assert allow_overflow or n_rec <= cap
     r = recs.cpu().numpy().view(np.uint32).reshape(-1, 3)[:min(n_rec, cap)]
+    # placeholders of samples whose records did not fit (count 0)
+    r = r[r[:, 2] != 0]
     order = np.lexsort((r[:, 0], r[:, 1]))  # by sample, then node
     r = r[order]
     nent = np.bincount(r[:, 1], minlength=count)
