@@ -88,12 +88,26 @@ __device__ void bucket_count(const RoundBuffers &rb, const ApplyArgs &a) {
         for (uint32_t s = a.lo + tid; s < a.hi; s += nth)
             rb.signs[s] = rademacher_mask(a.seed, a.first_sample + s);
     const uint32_t R = round_records(rb, a);
-    for (uint32_t i = tid; i < R; i += nth) {
-        PathRec r = rb.recs[i];
-        if (r.sample < a.lo || r.sample >= a.hi) continue;
-        if (atomicAdd(&rb.node_cnt[r.node], 1u) == 0u) {
-            uint32_t t = atomicAdd(rb.n_touched, 1u);
-            rb.touched[t] = r.node;
+    const uint32_t lane = threadIdx.x & 31;
+    // warp-uniform loop: the first record of a node is appended to the
+    // touched list with one counter increment per warp (a single counter
+    // that every warp hits would serialise the whole phase)
+    for (uint32_t i0 = tid - lane; i0 < R; i0 += nth) {
+        const uint32_t i = i0 + lane;
+        bool first = false;
+        uint32_t node = 0;
+        if (i < R) {
+            const PathRec r = rb.recs[i];
+            node = r.node;
+            if (r.sample >= a.lo && r.sample < a.hi)
+                first = atomicAdd(&rb.node_cnt[r.node], 1u) == 0u;
+        }
+        const uint32_t m = __ballot_sync(0xffffffffu, first);
+        if (m) {
+            uint32_t base = 0;
+            if (lane == 0) base = atomicAdd(rb.n_touched, (uint32_t)__popc(m));
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (first) rb.touched[base + __popc(m & ((1u << lane) - 1u))] = node;
         }
     }
 }
@@ -203,7 +217,46 @@ struct FoldScratch {
     double x[32];
     uint32_t signs[32];
     uint32_t sample[32];
+    uint32_t upd[32];  // nodes updated for the first time, not yet on upd_list
+    uint32_t nupd;
+    double sup_a, sup_w;  // the warp's maxima of approx and emp_wimpy_vars
 };
+
+// Per-warp folding state: reset before a warp's first fold, flushed after its
+// last (fold_flush), so that the job-wide maxima and the update list take one
+// global atomic per warp rather than one per node.
+__device__ __forceinline__ void fold_begin(FoldScratch &fs) {
+    if ((threadIdx.x & 31) == 0) {
+        fs.nupd = 0;
+        fs.sup_a = 0.0;
+        fs.sup_w = 0.0;
+    }
+    __syncwarp();
+}
+
+__device__ __forceinline__ void upd_flush(const JobCounters &jc, FoldScratch &fs) {
+    const uint32_t lane = threadIdx.x & 31;
+    __syncwarp();
+    const uint32_t k = fs.nupd;
+    if (k) {
+        uint32_t base = 0;
+        if (lane == 0) base = atomicAdd(&jc.sc->n_upd, k);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (lane < k) jc.upd_list[base + lane] = fs.upd[lane];
+        __syncwarp();
+        if (lane == 0) fs.nupd = 0;
+    }
+    __syncwarp();
+}
+
+__device__ __forceinline__ void fold_flush(const JobCounters &jc, FoldScratch &fs) {
+    upd_flush(jc, fs);
+    if ((threadIdx.x & 31) == 0) {
+        if (fs.sup_a > 0.) atomic_max_nonneg_double(&jc.sc->sup_approx_bits, fs.sup_a);
+        if (fs.sup_w > 0.) atomic_max_nonneg_double(&jc.sc->sup_wimpy_bits, fs.sup_w);
+    }
+    __syncwarp();
+}
 
 template <typename Get>
 __device__ void fold_node(const RoundBuffers &rb, const JobCounters &jc, const ApplyArgs &a,
@@ -236,11 +289,17 @@ __device__ void fold_node(const RoundBuffers &rb, const JobCounters &jc, const A
         const uint32_t kmax = min(32u, b - r0);
         if (lane < kTrials) {
             if (pass2) {
+                // (int64)((double)m + s x) with m kept as an integer-valued
+                // double: the conversions to and from int64 are exact (|m| is
+                // at most the sample count, far below 2^53), so truncating in
+                // double gives the same value with one dependent step fewer
+                double md = (double)m;
                 for (uint32_t k = 0; k < kmax; k++) {
                     const double x = fs.x[k];
                     const bool plus = (fs.signs[k] >> lane) & 1u;
-                    m = (long long)__double2ll_rz(__dadd_rn(__ll2double_rn(m), plus ? x : -x));
+                    md = trunc(__dadd_rn(md, plus ? x : -x));
                 }
+                m = (long long)md;
             }
         } else if (lane == 25) {
             for (uint32_t k = 0; k < kmax; k++) {
@@ -269,14 +328,16 @@ __device__ void fold_node(const RoundBuffers &rb, const JobCounters &jc, const A
     } else if (lane == 25) {
         jc.approx[node] = acc;
         if (lu) {
-            if (jc.last_upd[node] == 0) jc.upd_list[atomicAdd(&jc.sc->n_upd, 1u)] = node;
+            if (jc.last_upd[node] == 0) fs.upd[fs.nupd++] = node;
             jc.last_upd[node] = lu;
         }
-        atomic_max_nonneg_double(&jc.sc->sup_approx_bits, acc);
+        fs.sup_a = fmax(fs.sup_a, acc);
     } else if (lane == 26) {
         jc.wimpy[node] = acc;
-        atomic_max_nonneg_double(&jc.sc->sup_wimpy_bits, acc);
+        fs.sup_w = fmax(fs.sup_w, acc);
     }
+    __syncwarp();
+    if (fs.nupd == 32) upd_flush(jc, fs);
 }
 
 __device__ __forceinline__ void warp_bitonic_sort(unsigned long long &key) {
@@ -300,6 +361,9 @@ struct SmallSmem {
 };
 struct LargeSmem {
     unsigned long long sbuf[kLargeBucket];
+    uint32_t bits[kLargeBucket / 32];  // samples of the bucket
+    uint32_t wpre[kLargeBucket / 32];  // set bits before each word
+    uint32_t wsum[32];
     FoldScratch fsc;
 };
 constexpr size_t kCommitSmem = sizeof(LargeSmem) > sizeof(SmallSmem) ? sizeof(LargeSmem)
@@ -311,6 +375,7 @@ __device__ void apply_small(const RoundBuffers &rb, const JobCounters &jc, const
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const uint32_t gw = blockIdx.x * (blockDim.x >> 5) + wib;
     const uint32_t nw = gridDim.x * (blockDim.x >> 5);
+    fold_begin(sm.fsc[wib]);
     for (uint32_t t = gw; t < T; t += nw) {
         const uint32_t b0 = rb.bucket_off[t];
         const uint32_t b = rb.bucket_off[t + 1] - b0;
@@ -326,14 +391,21 @@ __device__ void apply_small(const RoundBuffers &rb, const JobCounters &jc, const
         fold_node(rb, jc, a, node, b, [&](uint32_t r) { return sm.buf[wib][r]; }, sm.fsc[wib]);
         __syncwarp();
     }
+    fold_flush(jc, sm.fsc[wib]);
 }
 
-// Buckets of more than 32 entries: one CTA per node, a bitonic sort in shared
-// memory (buckets are bounded by kLargeBucket through the sub-round size).
+// Buckets of more than 32 entries: one CTA per node.  The entries of a
+// bucket are distinct samples of the sub-round (a node is on a sample's path
+// map once), whose local index lies below kLargeBucket, so their order is
+// the rank of each sample in a bitmap of the sub-round: set one bit per
+// entry, prefix-count the bits per word, and each entry goes to its rank
+// (linear in the bucket; no comparison sort).
 __device__ void apply_large(const RoundBuffers &rb, const JobCounters &jc, const ApplyArgs &a,
                             LargeSmem &sm) {
     const uint32_t NL = __ldcg(rb.n_large);
     unsigned long long *sbuf = sm.sbuf;
+    constexpr uint32_t kWords = kLargeBucket / 32;
+    if (threadIdx.x < 32) fold_begin(sm.fsc);
     for (uint32_t li = blockIdx.x; li < NL; li += gridDim.x) {
         const uint32_t t = __ldcg(&rb.large[li]);
         const uint32_t b0 = rb.bucket_off[t];
@@ -342,33 +414,55 @@ __device__ void apply_large(const RoundBuffers &rb, const JobCounters &jc, const
             if (threadIdx.x == 0) atomicCAS(&jc.sc->error, 0, SILVAN_E_CAPACITY);
             continue;
         }
-        uint32_t P = 64;
-        while (P < b) P <<= 1;
-        for (uint32_t i = threadIdx.x; i < P; i += blockDim.x)
-            sbuf[i] = i < b ? rb.entries[b0 + i] : ~0ull;
+        for (uint32_t w = threadIdx.x; w < kWords; w += blockDim.x) sm.bits[w] = 0u;
         __syncthreads();
-        for (uint32_t k = 2; k <= P; k <<= 1) {
-            for (uint32_t j = k >> 1; j > 0; j >>= 1) {
-                for (uint32_t i = threadIdx.x; i < P; i += blockDim.x) {
-                    const uint32_t l = i ^ j;
-                    if (l > i) {
-                        const unsigned long long x = sbuf[i], y = sbuf[l];
-                        const bool asc = (i & k) == 0;
-                        if (asc ? (x > y) : (x < y)) {
-                            sbuf[i] = y;
-                            sbuf[l] = x;
-                        }
-                    }
+        for (uint32_t i = threadIdx.x; i < b; i += blockDim.x) {
+            const uint32_t sidx = (uint32_t)(rb.entries[b0 + i] >> 32) - a.lo;
+            if (sidx < kLargeBucket) atomicOr(&sm.bits[sidx >> 5], 1u << (sidx & 31));
+            else atomicCAS(&jc.sc->error, 0, SILVAN_E_STATE);
+        }
+        __syncthreads();
+        // exclusive prefix of the words' bit counts (one word per thread)
+        {
+            const uint32_t w = threadIdx.x;
+            const uint32_t c = w < kWords ? __popc(sm.bits[w]) : 0u;
+            uint32_t incl = c;
+            const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += v;
+            }
+            if (lane == 31) sm.wsum[warp] = incl;
+            __syncthreads();
+            if (warp == 0) {
+                const uint32_t v = lane < (int)(blockDim.x >> 5) ? sm.wsum[lane] : 0u;
+                uint32_t vi = v;
+                for (int o = 1; o < 32; o <<= 1) {
+                    const uint32_t u = __shfl_up_sync(0xffffffffu, vi, o);
+                    if (lane >= o) vi += u;
                 }
-                __syncthreads();
+                sm.wsum[lane] = vi - v;
+            }
+            __syncthreads();
+            if (w < kWords) sm.wpre[w] = sm.wsum[warp] + incl - c;
+        }
+        __syncthreads();
+        for (uint32_t i = threadIdx.x; i < b; i += blockDim.x) {
+            const unsigned long long e = rb.entries[b0 + i];
+            const uint32_t sidx = (uint32_t)(e >> 32) - a.lo;
+            if (sidx < kLargeBucket) {
+                const uint32_t w = sidx >> 5;
+                sbuf[sm.wpre[w] + __popc(sm.bits[w] & ((1u << (sidx & 31)) - 1u))] = e;
             }
         }
+        __syncthreads();
         if (threadIdx.x < 32) {
             const uint32_t node = rb.touched[t];
             fold_node(rb, jc, a, node, b, [&](uint32_t r) { return sbuf[r]; }, sm.fsc);
         }
         __syncthreads();
     }
+    if (threadIdx.x < 32) fold_flush(jc, sm.fsc);
 }
 
 __device__ void commit_sums(const RoundBuffers &rb, const JobCounters &jc, const ApplyArgs &a) {
@@ -398,13 +492,26 @@ __device__ void commit_sums(const RoundBuffers &rb, const JobCounters &jc, const
         ball += __shfl_xor_sync(0xffffffffu, ball, o);
         pred += __shfl_xor_sync(0xffffffffu, pred, o);
     }
+    // per CTA in shared memory, then one global add per CTA and sum
+    __shared__ unsigned long long cs[6];
+    if (threadIdx.x < 6) cs[threadIdx.x] = 0ull;
+    __syncthreads();
     if ((threadIdx.x & 31) == 0) {
-        if (vis) atomicAdd(&jc.sc->vis_edges, vis);
-        if (cnt) atomicAdd(&jc.sc->counted_samples, cnt);
-        if (vd) atomicAdd(&jc.sc->void_samples, vd);
-        if (paths) atomicAdd(&jc.sc->paths, paths);
-        if (ball) atomicAdd(&jc.sc->ball_nodes, ball);
-        if (pred) atomicAdd(&jc.sc->pred_entries, pred);
+        if (vis) atomicAdd(&cs[0], vis);
+        if (cnt) atomicAdd(&cs[1], cnt);
+        if (vd) atomicAdd(&cs[2], vd);
+        if (paths) atomicAdd(&cs[3], paths);
+        if (ball) atomicAdd(&cs[4], ball);
+        if (pred) atomicAdd(&cs[5], pred);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (cs[0]) atomicAdd(&jc.sc->vis_edges, cs[0]);
+        if (cs[1]) atomicAdd(&jc.sc->counted_samples, cs[1]);
+        if (cs[2]) atomicAdd(&jc.sc->void_samples, cs[2]);
+        if (cs[3]) atomicAdd(&jc.sc->paths, cs[3]);
+        if (cs[4]) atomicAdd(&jc.sc->ball_nodes, cs[4]);
+        if (cs[5]) atomicAdd(&jc.sc->pred_entries, cs[5]);
     }
 }
 

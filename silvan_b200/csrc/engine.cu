@@ -1535,9 +1535,11 @@ bool Job::next_request(JobRequest &r) {
                                           : std::min<uint64_t>(lookahead_tail_, 4 * target_);
         if (phase_ == kPass1 && hint_total_ > target_) {
             // the last job of this class of graphs used hint_total_ samples
-            // with pass 2 on the same stream: draw that far at once (10 %
-            // more), so that one launch usually covers the whole estimation
-            ahead = std::max<uint64_t>(ahead, hint_total_ + hint_total_ / 10 - target_);
+            // with pass 2 on the same stream: draw that far at once (25 %
+            // more: the stop of another seed lies within a schedule step or
+            // two, and a second launch costs more than the extra samples),
+            // so that one launch usually covers the whole estimation
+            ahead = std::max<uint64_t>(ahead, hint_total_ + hint_total_ / 4 - target_);
         }
         if (phase_ == kPass2 && predicted_stop_ > pass_samples_) {
             // absolute mode after a failed check: up to the schedule point at

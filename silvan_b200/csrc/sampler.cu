@@ -735,8 +735,16 @@ __device__ __forceinline__ int32_t post_level(const SamplerLaunch &L, SamplerSme
     const uint2 r0 = drows[x0];
     const uint32_t items = depth == 0 ? r0.y - r0.x : (side_u ? s.sum_u : s.sum_v);
     const uint32_t F = hi - lo;
-    const uint32_t thr =
-        A.assist_items == kAssistItemsAuto ? 8u * (uint32_t)Shape<BLOCK>::kTile : A.assist_items;
+    // Default threshold: eight tiles while the round still has samples to
+    // hand out (CTAs are busy and help only between levels), two tiles once
+    // every sample is taken: then the CTAs that ran out of samples are idle
+    // until the launch ends, and the last samples' levels are what they wait
+    // for.
+    uint32_t thr = A.assist_items;
+    if (thr == kAssistItemsAuto) {
+        const bool draining = ld_acquire_u32(&L.hdr->work) >= L.hdr->total;
+        thr = (draining ? 2u : 8u) * (uint32_t)Shape<BLOCK>::kTile;
+    }
     if (items < thr || F > L.assist.node_cap ||
         (uint64_t)items / Shape<BLOCK>::kTile + F / Shape<BLOCK>::kChunk + 2u > L.assist.tile_cap)
         return -1;
@@ -1279,7 +1287,7 @@ __global__ void __launch_bounds__(BLOCK, Shape<BLOCK>::kMinBlocks) sampler_kerne
                     pick = -2;
                 } else {
                     __nanosleep(s.a_nap);
-                    s.a_nap = min(s.a_nap * 2u, 16384u);
+                    s.a_nap = min(s.a_nap * 2u, 4096u);
                 }
             } else {
                 s.a_nap = 256;
