@@ -81,8 +81,9 @@ typedef struct {
     uint32_t backtrack;  /* SILVAN_BACKTRACK_*                               */
     uint32_t assist_items; /* BFS levels of at least this many adjacency
                             entries are expanded by several sampler CTAs
-                            together (same results): 0 = default (32 x the
-                            CTA size: eight tiles), 0xffffffff = never      */
+                            together (same results): 0 = default (128 x the
+                            CTA size while samples remain to be handed out,
+                            8 x once all are taken), 0xffffffff = never     */
     uint32_t wait_polls; /* polls after which a wait between the CTAs that
                             share a level gives up (the sample then reports
                             SILVAN_E_TIMEOUT and the job fails; later jobs

@@ -159,6 +159,13 @@ __device__ __forceinline__ void rec_reset(NodeRec *r) {
                  : "memory");
 }
 
+// A whole record in one 32-byte store.
+__device__ __forceinline__ void rec_store(NodeRec *r, uint4 lo, uint4 hi) {
+    asm volatile("st.global.v8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"l"(r), "r"(lo.x),
+                 "r"(lo.y), "r"(lo.z), "r"(lo.w), "r"(hi.x), "r"(hi.y), "r"(hi.z), "r"(hi.w)
+                 : "memory");
+}
+
 // A whole record in one 32-byte load through L2 (the slot is written by this
 // CTA and, for shared levels, by others): words 0-3 and 4-7.
 __device__ __forceinline__ void rec_load(const NodeRec *r, uint4 &lo, uint4 &hi) {
@@ -406,6 +413,13 @@ __device__ void expand_level(const SegDesc &A, SamplerSmem<BLOCK> &s, NodeRec *r
                 else if (st_side(sty[k]) != side) code[k] = 2;
                 else code[k] = 0;
             }
+            // Phase 1 records only the hit count and the smallest key.  Most
+            // new nodes of a level have a single hit (about 1.2 hits per node
+            // on R-MAT); their whole record is then written by the joining
+            // hit with one store in phase 2, and only nodes with several hits
+            // get the sigma and last-key atomics.  The tiles of a level run
+            // one after another on this CTA, so a later tile's hits find the
+            // record complete and add to it.
 #pragma unroll
             for (int k = 0; k < kItems; k++) {
                 if (code[k] != 1) continue;
@@ -413,27 +427,29 @@ __device__ void expand_level(const SegDesc &A, SamplerSmem<BLOCK> &s, NodeRec *r
                 const unsigned long long key = ((unsigned long long)(gbase + it) << 32) | xs[k];
                 NodeRec *r = &rec[ys[k]];
                 atomicMin(reinterpret_cast<unsigned long long *>(&r->first), key);
-                atomicMax(reinterpret_cast<unsigned long long *>(&r->last), key);
                 atomicAdd(&r->cnt, 1u);
-                atomicAdd(reinterpret_cast<unsigned long long *>(&r->sigma), s.f_sig[li[k]]);
             }
             __syncthreads();
             // ---- phase 2: ordered compaction of joins and meeting edges -------
-            unsigned long long fv[kItems];
-#pragma unroll
-            for (int k = 0; k < kItems; k++)
-                fv[k] = code[k] == 1
-                            ? __ldcg(reinterpret_cast<const unsigned long long *>(&rec[ys[k]].first))
-                            : 0ull;
-            uint32_t rn[kItems], rm[kItems];
+            uint32_t single = 0;  // bit k: item k is the node's only hit so far
 #pragma unroll
             for (int k = 0; k < kItems; k++) {
+                if (code[k] != 1) continue;
+                uint4 lo4, hi4;
+                rec_load(&rec[ys[k]], lo4, hi4);
                 const uint32_t it = t0 + (uint32_t)(k * BLOCK) + threadIdx.x;
-                if (code[k] == 1) {
-                    hits_local++;
-                    if ((uint32_t)(fv[k] >> 32) != gbase + it) code[k] = 0;
+                const unsigned long long key = ((unsigned long long)(gbase + it) << 32) | xs[k];
+                hits_local++;
+                if (lo4.y > 1u) {  // several hits: sigma and the last key by atomics
+                    NodeRec *r = &rec[ys[k]];
+                    atomicMax(reinterpret_cast<unsigned long long *>(&r->last), key);
+                    atomicAdd(reinterpret_cast<unsigned long long *>(&r->sigma), s.f_sig[li[k]]);
+                } else {
+                    single |= 1u << k;
                 }
+                if (hi4.y != gbase + it) code[k] = 0;  // not the joining hit
             }
+            uint32_t rn[kItems], rm[kItems];
 #pragma unroll
             for (int k = 0; k < kItems; k++) {
                 const uint32_t bn = __ballot_sync(0xffffffffu, code[k] == 1);
@@ -499,7 +515,15 @@ __device__ void expand_level(const SegDesc &A, SamplerSmem<BLOCK> &s, NodeRec *r
                 if (code[k] == 1) {
                     const uint32_t y = ys[k];
                     queue[s.warp_a[k * kWarps + warp] + rn[k]] = y;
-                    rec[y].st = new_st;
+                    if (single & (1u << k)) {
+                        // the only hit: st, cnt = 1, sigma, first = last = key
+                        const uint32_t it = t0 + (uint32_t)(k * BLOCK) + threadIdx.x;
+                        const unsigned long long sg = s.f_sig[li[k]];
+                        rec_store(&rec[y], make_uint4(new_st, 1u, (uint32_t)sg, (uint32_t)(sg >> 32)),
+                                  make_uint4(xs[k], gbase + it, xs[k], gbase + it));
+                    } else {
+                        rec[y].st = new_st;
+                    }
                     sum_local += dg[k];
                 } else if (code[k] == 2) {
                     const uint32_t pos = s.warp_b[k * kWarps + warp] + rm[k];
@@ -735,15 +759,17 @@ __device__ __forceinline__ int32_t post_level(const SamplerLaunch &L, SamplerSme
     const uint2 r0 = drows[x0];
     const uint32_t items = depth == 0 ? r0.y - r0.x : (side_u ? s.sum_u : s.sum_v);
     const uint32_t F = hi - lo;
-    // Default threshold: eight tiles while the round still has samples to
-    // hand out (CTAs are busy and help only between levels), two tiles once
-    // every sample is taken: then the CTAs that ran out of samples are idle
-    // until the launch ends, and the last samples' levels are what they wait
-    // for.
+    // Default threshold: 32 tiles while the round still has samples to hand
+    // out, two tiles once every sample is taken.  While samples remain, every
+    // CTA is busy with its own and helps only between samples, and a shared
+    // tile costs more than one expanded alone (the look-backs and the tile
+    // table), so only levels long enough to become the launch's tail are
+    // shared; once the round is drained, the CTAs without samples are idle
+    // and the last samples' levels are what the launch waits for.
     uint32_t thr = A.assist_items;
     if (thr == kAssistItemsAuto) {
         const bool draining = ld_acquire_u32(&L.hdr->work) >= L.hdr->total;
-        thr = (draining ? 2u : 8u) * (uint32_t)Shape<BLOCK>::kTile;
+        thr = (draining ? 2u : 32u) * (uint32_t)Shape<BLOCK>::kTile;
     }
     if (items < thr || F > L.assist.node_cap ||
         (uint64_t)items / Shape<BLOCK>::kTile + F / Shape<BLOCK>::kChunk + 2u > L.assist.tile_cap)
@@ -1382,19 +1408,6 @@ __global__ void __launch_bounds__(BLOCK, Shape<BLOCK>::kMinBlocks) sampler_kerne
         // ---- balanced bidirectional BFS (:89-144) ------------------------------
         uint32_t exp_side = kSideU;
         for (;;) {
-            // Levels that other samples posted on the board come before this
-            // sample's next level: a wide level ends sooner the more CTAs
-            // take its tiles, and the launch lasts as long as its slowest
-            // sample.  (Nothing of this sample's state is touched meanwhile.)
-            if (L.assist.entries != nullptr) {
-                for (;;) {
-                    if (threadIdx.x == 0) s.a_entry = join_entry<BLOCK>(L, s, blockIdx.x);
-                    __syncthreads();
-                    if (s.a_entry < 0) break;
-                    help_entry<BLOCK>(L, s, (uint32_t)s.a_entry);
-                    __syncthreads();
-                }
-            }
             const bool side_u = s.sum_u <= s.sum_v;
             exp_side = side_u ? kSideU : kSideV;
             const uint32_t lo = side_u ? s.start_u : s.start_v;

@@ -13,7 +13,8 @@ constexpr int kSamplerBlock = 512;   // default threads per slot
 constexpr int kSamplerBlocks[4] = {128, 256, 512, 1024};  // compiled CTA sizes
 constexpr uint32_t kMeetCap = 1u << 16;  // meeting edges per sample
 // SegDesc::assist_items value for the default threshold: levels of at least
-// eight tiles of the launch's CTA size (32 x CTA-size adjacency entries)
+// 32 tiles of the launch's CTA size while the round has samples left, two
+// tiles once it is drained
 constexpr uint32_t kAssistItemsAuto = 0xffffffffu;
 
 // One job's share of a sampler launch: samples [first_sample, first_sample +
