@@ -26,16 +26,15 @@ namespace {
 // ---------------------------------------------------------------------------
 // One commit round as a single cooperative kernel.  Its phases are separated
 // by grid-wide barriers (every CTA is resident: cooperative launch):
-//   A  the round's Rademacher signs (pass 2); records counted per node and
-//      the touched nodes listed
-//   B  per-CTA sums of the counts over a contiguous range of the list
-//   C  exclusive scan of the counts (each CTA adds the sums of the CTAs
-//      before it), the bucket offsets and the scatter cursors
-//   D  records scattered into their nodes' buckets
-//   E  buckets of at most 32 entries sorted and folded by one warp each
-//      (larger ones listed); the round's scalar sums; cursors zeroed
-//   F  buckets of more than 32 entries sorted in shared memory and folded,
-//      one CTA each
+//   A  per sample the Rademacher signs (pass 2) and 1 / num_paths; records
+//      counted per node and the touched nodes listed
+//   B  bucket space of every touched node taken from a cursor (warp
+//      aggregated), the scatter cursors, the list of buckets of more than
+//      32 entries
+//   C  records scattered into their nodes' buckets
+//   D  the large buckets (one CTA each, claimed from a cursor), then the
+//      small ones (one warp each, eight nodes per claim); the round's scalar
+//      sums; cursors zeroed
 // Each barrier is bounded: a CTA that waits longer than kBarrierPolls polls
 // records SILVAN_E_TIMEOUT in the job's error word and leaves the kernel.
 // ---------------------------------------------------------------------------
@@ -84,9 +83,12 @@ __device__ bool grid_barrier(uint32_t *bar) {
 
 __device__ void bucket_count(const RoundBuffers &rb, const ApplyArgs &a) {
     const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
-    if (a.pass == 2)
-        for (uint32_t s = a.lo + tid; s < a.hi; s += nth)
-            rb.signs[s] = rademacher_mask(a.seed, a.first_sample + s);
+    // per sample: the Rademacher signs (pass 2) and 1 / num_paths, the factor
+    // every record of the sample is multiplied by (Probabilistic.cpp:502)
+    for (uint32_t s = a.lo + tid; s < a.hi; s += nth) {
+        if (a.pass == 2) rb.signs[s] = rademacher_mask(a.seed, a.first_sample + s);
+        rb.inv_np[s] = __ddiv_rn(1.0, (double)rb.np[s]);
+    }
     const uint32_t R = round_records(rb, a);
     const uint32_t lane = threadIdx.x & 31;
     // warp-uniform loop: the first record of a node is appended to the
@@ -112,84 +114,40 @@ __device__ void bucket_count(const RoundBuffers &rb, const ApplyArgs &a) {
     }
 }
 
-// Contiguous range of the touched list owned by this CTA.
-__device__ __forceinline__ void range_of(uint32_t T, uint32_t &b, uint32_t &e) {
-    uint32_t per = (T + gridDim.x - 1) / gridDim.x;
-    b = min(T, blockIdx.x * per);
-    e = min(T, b + per);
-}
-
-__device__ void scan_reduce(const RoundBuffers &rb, uint32_t T, uint32_t *tmp) {
-    uint32_t b, e;
-    range_of(T, b, e);
-    uint32_t v = 0;
-    for (uint32_t i = b + threadIdx.x; i < e; i += blockDim.x) v += rb.node_cnt[rb.touched[i]];
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    if ((threadIdx.x & 31) == 0) tmp[threadIdx.x >> 5] = v;
-    __syncthreads();
-    if (threadIdx.x < 32) {
-        uint32_t t = threadIdx.x < (blockDim.x >> 5) ? tmp[threadIdx.x] : 0u;
-        for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
-        if (threadIdx.x == 0) rb.block_sums[blockIdx.x] = t;
-    }
-    __syncthreads();
-}
-
-__device__ void scan_down(const RoundBuffers &rb, uint32_t T, uint32_t *tmp) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    // the sums of the CTAs before this one (warp 0), and of all CTAs
-    if (warp == 0) {
-        uint32_t before = 0, all = 0;
-        for (uint32_t i = lane; i < gridDim.x; i += 32) {
-            const uint32_t v = __ldcg(&rb.block_sums[i]);
-            all += v;
-            if (i < blockIdx.x) before += v;
+// Bucket space of every touched node, taken from a cursor (the buckets need
+// no order among themselves): one atomic per warp for the warp's nodes, the
+// lanes' offsets by a warp scan.  The node's count becomes its scatter
+// cursor; buckets of more than 32 entries are listed for the CTA-wide fold.
+__device__ void bucket_alloc(const RoundBuffers &rb, uint32_t T) {
+    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
+    const uint32_t lane = threadIdx.x & 31;
+    for (uint32_t t0 = tid - lane; t0 < T; t0 += nth) {
+        const uint32_t t = t0 + lane;
+        uint32_t node = 0, b = 0;
+        if (t < T) {
+            node = rb.touched[t];
+            b = rb.node_cnt[node];
         }
-        for (int o = 16; o > 0; o >>= 1) {
-            before += __shfl_xor_sync(0xffffffffu, before, o);
-            all += __shfl_xor_sync(0xffffffffu, all, o);
-        }
-        if (lane == 0) {
-            tmp[33] = before;
-            if (blockIdx.x == gridDim.x - 1) rb.bucket_off[T] = all;
-        }
-    }
-    __syncthreads();
-    uint32_t carry = tmp[33];
-    uint32_t b, e;
-    range_of(T, b, e);
-    for (uint32_t c0 = b; c0 < e; c0 += blockDim.x) {
-        const uint32_t i = c0 + threadIdx.x;
-        uint32_t node = 0, v = 0;
-        if (i < e) {
-            node = rb.touched[i];
-            v = rb.node_cnt[node];
-        }
-        uint32_t incl = v;
+        uint32_t incl = b;
         for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += t;
+            const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += v;
         }
-        if (lane == 31) tmp[warp] = incl;
-        __syncthreads();
-        if (warp == 0) {
-            const uint32_t w = lane < nw ? tmp[lane] : 0u;
-            uint32_t wi = w;
-            for (int o = 1; o < 32; o <<= 1) {
-                const uint32_t t = __shfl_up_sync(0xffffffffu, wi, o);
-                if (lane >= o) wi += t;
-            }
-            if (lane < nw) tmp[lane] = wi - w;
-            if (lane == 31) tmp[32] = wi;
+        uint32_t base = 0;
+        if (lane == 31 && incl) base = atomicAdd(rb.n_touched + 4, incl);
+        base = __shfl_sync(0xffffffffu, base, 31);
+        const bool large = b > 32;
+        const uint32_t lm = __ballot_sync(0xffffffffu, large);
+        uint32_t lbase = 0;
+        if (lm && lane == 0) lbase = atomicAdd(rb.n_large, (uint32_t)__popc(lm));
+        lbase = __shfl_sync(0xffffffffu, lbase, 0);
+        if (t < T) {
+            const uint32_t off = base + incl - b;
+            rb.bucket_off[t] = off;
+            rb.bucket_len[t] = b;
+            rb.node_cnt[node] = off;  // becomes the scatter cursor
+            if (large) rb.large[lbase + __popc(lm & ((1u << lane) - 1u))] = t;
         }
-        __syncthreads();
-        const uint32_t excl = carry + tmp[warp] + incl - v;
-        if (i < e) {
-            rb.bucket_off[i] = excl;
-            rb.node_cnt[node] = excl;  // becomes the scatter cursor
-        }
-        carry += tmp[32];
-        __syncthreads();
     }
 }
 
@@ -281,7 +239,7 @@ __device__ void fold_node(const RoundBuffers &rb, const JobCounters &jc, const A
             const unsigned long long e = get(r);
             const uint32_t sl = (uint32_t)(e >> 32);
             const uint32_t c = (uint32_t)e;
-            fs.x[lane] = __dmul_rn((double)c, __ddiv_rn(1.0, (double)rb.np[sl]));
+            fs.x[lane] = __dmul_rn((double)c, rb.inv_np[sl]);
             fs.signs[lane] = pass2 ? rb.signs[sl] : 0u;
             fs.sample[lane] = sl;
         }
@@ -369,32 +327,36 @@ struct LargeSmem {
 constexpr size_t kCommitSmem = sizeof(LargeSmem) > sizeof(SmallSmem) ? sizeof(LargeSmem)
                                                                         : sizeof(SmallSmem);
 
-// Buckets of at most 32 entries: one warp per node; larger ones are listed.
+// Buckets of at most 32 entries: one warp per node, eight touched nodes per
+// claim of the round's cursor (larger buckets are skipped: the CTA-wide fold
+// takes them).
 __device__ void apply_small(const RoundBuffers &rb, const JobCounters &jc, const ApplyArgs &a,
                             uint32_t T, SmallSmem &sm) {
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    const uint32_t gw = blockIdx.x * (blockDim.x >> 5) + wib;
-    const uint32_t nw = gridDim.x * (blockDim.x >> 5);
     fold_begin(sm.fsc[wib]);
-    for (uint32_t t = gw; t < T; t += nw) {
-        const uint32_t b0 = rb.bucket_off[t];
-        const uint32_t b = rb.bucket_off[t + 1] - b0;
-        if (b > 32) {
-            if (lane == 0) rb.large[atomicAdd(rb.n_large, 1u)] = t;
-            continue;
+    for (;;) {
+        uint32_t t0 = 0;
+        if (lane == 0) t0 = atomicAdd(rb.n_touched + 6, 8u);
+        t0 = __shfl_sync(0xffffffffu, t0, 0);
+        if (t0 >= T) break;
+        for (uint32_t t = t0; t < min(T, t0 + 8u); t++) {
+            const uint32_t b = rb.bucket_len[t];
+            if (b > 32) continue;
+            const uint32_t b0 = rb.bucket_off[t];
+            const uint32_t node = rb.touched[t];
+            unsigned long long key = (uint32_t)lane < b ? rb.entries[b0 + lane] : ~0ull;
+            warp_bitonic_sort(key);
+            sm.buf[wib][lane] = key;
+            __syncwarp();
+            fold_node(rb, jc, a, node, b, [&](uint32_t r) { return sm.buf[wib][r]; },
+                      sm.fsc[wib]);
+            __syncwarp();
         }
-        const uint32_t node = rb.touched[t];
-        unsigned long long key = (uint32_t)lane < b ? rb.entries[b0 + lane] : ~0ull;
-        warp_bitonic_sort(key);
-        sm.buf[wib][lane] = key;
-        __syncwarp();
-        fold_node(rb, jc, a, node, b, [&](uint32_t r) { return sm.buf[wib][r]; }, sm.fsc[wib]);
-        __syncwarp();
     }
     fold_flush(jc, sm.fsc[wib]);
 }
 
-// Buckets of more than 32 entries: one CTA per node.  The entries of a
+// Buckets of more than 32 entries: one CTA per node, claimed from a cursor.  The entries of a
 // bucket are distinct samples of the sub-round (a node is on a sample's path
 // map once), whose local index lies below kLargeBucket, so their order is
 // the rank of each sample in a bitmap of the sub-round: set one bit per
@@ -405,11 +367,17 @@ __device__ void apply_large(const RoundBuffers &rb, const JobCounters &jc, const
     const uint32_t NL = __ldcg(rb.n_large);
     unsigned long long *sbuf = sm.sbuf;
     constexpr uint32_t kWords = kLargeBucket / 32;
+    __shared__ uint32_t claim;
     if (threadIdx.x < 32) fold_begin(sm.fsc);
-    for (uint32_t li = blockIdx.x; li < NL; li += gridDim.x) {
+    for (;;) {
+        if (threadIdx.x == 0) claim = atomicAdd(rb.n_touched + 5, 1u);
+        __syncthreads();
+        const uint32_t li = claim;
+        __syncthreads();
+        if (li >= NL) break;
         const uint32_t t = __ldcg(&rb.large[li]);
         const uint32_t b0 = rb.bucket_off[t];
-        const uint32_t b = rb.bucket_off[t + 1] - b0;
+        const uint32_t b = rb.bucket_len[t];
         if (b > kLargeBucket) {
             if (threadIdx.x == 0) atomicCAS(&jc.sc->error, 0, SILVAN_E_CAPACITY);
             continue;
@@ -527,20 +495,21 @@ __global__ void __launch_bounds__(kCommitThreads, 1) commit_round_kernel(const A
     if (!grid_barrier(bar)) goto timeout;
     {
         const uint32_t T = __ldcg(rb.n_touched);
-        scan_reduce(rb, T, tmp);
-        if (!grid_barrier(bar)) goto timeout;
-        scan_down(rb, T, tmp);
+        bucket_alloc(rb, T);
         if (!grid_barrier(bar)) goto timeout;
         bucket_scatter(rb, a);
         if (!grid_barrier(bar)) goto timeout;
+        // the large buckets first (CTA-wide, few), then the small ones
+        // (one warp each): the CTAs without a large bucket start on the
+        // small ones at once
+        apply_large(rb, jc, a, *reinterpret_cast<LargeSmem *>(commit_smem));
+        __syncthreads();
         apply_small(rb, jc, a, T, *reinterpret_cast<SmallSmem *>(commit_smem));
         commit_sums(rb, jc, a);
         // the scatter cursors back to zero for the next round
         for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < T;
              t += gridDim.x * blockDim.x)
             rb.node_cnt[rb.touched[t]] = 0;
-        if (!grid_barrier(bar)) goto timeout;
-        apply_large(rb, jc, a, *reinterpret_cast<LargeSmem *>(commit_smem));
     }
     return;
 timeout:
@@ -570,8 +539,8 @@ cudaError_t apply_init() {
 
 cudaError_t apply_round(const ApplyState *st, uint32_t *n_touched, cudaStream_t stream) {
     if (g_commit_grid <= 0) return cudaErrorNotReady;
-    // n_touched, n_large and the barrier's two words
-    cudaError_t e = cudaMemsetAsync(n_touched, 0, 4 * sizeof(uint32_t), stream);
+    // the round's control words (see RoundBuffers::n_touched)
+    cudaError_t e = cudaMemsetAsync(n_touched, 0, 8 * sizeof(uint32_t), stream);
     if (e != cudaSuccess) return e;
     cudaLaunchConfig_t cfg{};
     cfg.gridDim = dim3((unsigned)g_commit_grid);

@@ -38,6 +38,7 @@ struct RoundBuffers {
     uint32_t *signs;
     uint32_t *ball;
     uint32_t *pred;
+    double *inv_np;  // 1 / num_paths of each sample (set by the commit)
     uint32_t max_samples;
     // path-map records
     PathRec *recs;
@@ -46,12 +47,15 @@ struct RoundBuffers {
     // bucketing by node
     uint32_t *node_cnt;      // n, zero between rounds
     uint32_t *touched;       // distinct nodes of the round
-    uint32_t *n_touched;     // [0] touched nodes, [1] large buckets, [2..3] grid barrier
-    uint32_t *bucket_off;    // n_touched + 1
+    // control words of a commit round, zeroed before it: [0] touched nodes,
+    // [1] large buckets, [2..3] grid barrier, [4] bucket-space cursor,
+    // [5] large-bucket claims, [6] small-bucket claims, [7] unused
+    uint32_t *n_touched;
+    uint32_t *bucket_off;    // start of each touched node's bucket
+    uint32_t *bucket_len;    // its number of entries
     uint32_t *large;         // buckets of more than 32 entries (listed by apply_small)
     uint32_t *n_large;       // = n_touched + 1 (both zeroed together)
     unsigned long long *entries;  // sample << 32 | count, grouped by node
-    uint32_t *block_sums;    // scan scratch
     uint32_t *work_counter;  // sampler work counter
 };
 
@@ -95,8 +99,8 @@ constexpr int kApplyRoundKernels = 1;
 // counters, all read from `st` on the device: one cooperative kernel whose
 // phases are separated by grid-wide barriers.  Launches only, with a fixed
 // grid, so it can be captured in a CUDA graph.  n_touched is the RoundBuffers
-// field of the same struct (4 words: touched nodes, large buckets and the
-// grid barrier's two words, zeroed here before the kernel).
+// field of the same struct (its eight control words are zeroed here before
+// the kernel).
 cudaError_t apply_round(const ApplyState *st, uint32_t *n_touched, cudaStream_t stream);
 // Function attributes and resident grid of the commit kernel on the current
 // device (call before capturing).

@@ -918,14 +918,15 @@ Job::~Job() {
     dfree(r.signs);
     dfree(r.ball);
     dfree(r.pred);
+    dfree(r.inv_np);
     dfree(r.recs);
     dfree(r.node_cnt);
     dfree(r.touched);
     dfree(r.large);
     dfree(r.n_touched);
     dfree(r.bucket_off);
+    dfree(r.bucket_len);
     dfree(r.entries);
-    dfree(r.block_sums);
     dfree(jc_.approx);
     dfree(jc_.wimpy);
     dfree(jc_.mcrade);
@@ -969,9 +970,9 @@ int Job::alloc_round(uint32_t max_samples, uint64_t rec_cap) {
     RK(dmalloc(&r.ball, max_samples));
     RK(dmalloc(&r.pred, max_samples));
     RK(dmalloc(&r.node_cnt, n_));
-    RK(dmalloc(&r.n_touched, 4));
+    RK(dmalloc(&r.n_touched, 8));
+    RK(dmalloc(&r.inv_np, max_samples));
     r.n_large = r.n_touched + 1;
-    RK(dmalloc(&r.block_sums, 1024));
     r.rec_cursor = nullptr;
     r.work_counter = nullptr;
     CK(cudaMemset(r.node_cnt, 0, sizeof(uint32_t) * n_));
@@ -985,6 +986,7 @@ int Job::grow_records(uint64_t cap) {
     dfree(r.touched);
     dfree(r.large);
     dfree(r.bucket_off);
+    dfree(r.bucket_len);
     dfree(r.entries);
     r.rec_cap = cap;
     const uint64_t tcap = std::min<uint64_t>(cap, n_) + 1;
@@ -992,6 +994,7 @@ int Job::grow_records(uint64_t cap) {
     RK(dmalloc(&r.touched, tcap));
     RK(dmalloc(&r.large, tcap));
     RK(dmalloc(&r.bucket_off, tcap + 1));
+    RK(dmalloc(&r.bucket_len, tcap));
     RK(dmalloc(&r.entries, cap));
     return SILVAN_OK;
 }
