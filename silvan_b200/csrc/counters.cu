@@ -7,11 +7,12 @@
 //   mcrade[u][j] = (int64)((double)mcrade[u][j] + sign_j * x)   (truncation)
 // With num_paths > 1 the additions are not associative, so a node's updates
 // must be applied in sample order.  A round's records are grouped by node
-// (count, scan, scatter), each node's group is sorted by sample index (a warp
-// bitonic sort for groups of <= 32, a CTA sort in shared memory otherwise)
-// and the group is folded sequentially: lanes 0..24 each carry one Monte
-// Carlo trial, lane 25 approx, lane 26 the wimpy variance.  Different nodes
-// are independent, so the only serial work is per node.
+// (count, bucket space, scatter), each node's group is put in sample order
+// (by rank: compares for groups of <= 32, a bitmap of the sub-round's samples
+// otherwise) and the group is folded sequentially by one warp: lanes 0..24
+// each carry one Monte Carlo trial, lane 25 approx, lane 26 the wimpy
+// variance.  Different nodes are independent, so the only serial work is per
+// node.
 #include <algorithm>
 #include <cfloat>
 #include <cstring>
@@ -32,8 +33,9 @@ namespace {
 //      aggregated), the scatter cursors, the list of buckets of more than
 //      32 entries
 //   C  records scattered into their nodes' buckets
-//   D  the large buckets (one CTA each, claimed from a cursor), then the
-//      small ones (one warp each, eight nodes per claim); the round's scalar
+//   D  the sub-round's 1 / num_paths and signs staged in shared memory;
+//      the large buckets on warp 0 of each CTA (claimed from a cursor), the
+//      small ones on the other warps (fixed assignment); the round's scalar
 //      sums; cursors zeroed
 // Each barrier is bounded: a CTA that waits longer than kBarrierPolls polls
 // records SILVAN_E_TIMEOUT in the job's error word and leaves the kernel.
@@ -161,16 +163,13 @@ __device__ void bucket_scatter(const RoundBuffers &rb, const ApplyArgs &a) {
         rb.entries[pos] = ((unsigned long long)r.sample << 32) | r.count;
     }
 }
-__device__ __forceinline__ void atomic_max_nonneg_double(unsigned long long *p, double v) {
-    atomicMax(p, (unsigned long long)__double_as_longlong(v));
-}
-
-// Sequential fold of one node's sorted contributions.  Lane j < 25 carries
-// trial j of mcrade, lane 25 approx (and the top-k mark), lane 26 the wimpy
-// variance.  get(r) returns the r-th (sample << 32 | count) entry.  Entries
-// are prepared 32 at a time by all lanes (x = count * (1/num_paths) and the
-// sample's signs, into the warp's shared scratch) so that the sequential
-// chains only read shared memory.
+// Sequential fold of one node's contributions in sample order.  Every lane
+// runs the same instruction stream and carries one chain: lane j < 25 trial j
+// of mcrade, lane 25 approx (and the top-k crossing), lane 26 the wimpy
+// variance; lanes 27..31 repeat lane 25's chain and store nothing.  The chains
+// advance together, one entry per step.  The entries are staged 32 at a time
+// in the warp's scratch: x = count * (1 / num_paths), the sample's signs and
+// its round-local index.
 struct FoldScratch {
     double x[32];
     uint32_t signs[32];
@@ -207,6 +206,10 @@ __device__ __forceinline__ void upd_flush(const JobCounters &jc, FoldScratch &fs
     __syncwarp();
 }
 
+__device__ __forceinline__ void atomic_max_nonneg_double(unsigned long long *p, double v) {
+    atomicMax(p, (unsigned long long)__double_as_longlong(v));
+}
+
 __device__ __forceinline__ void fold_flush(const JobCounters &jc, FoldScratch &fs) {
     upd_flush(jc, fs);
     if ((threadIdx.x & 31) == 0) {
@@ -216,221 +219,210 @@ __device__ __forceinline__ void fold_flush(const JobCounters &jc, FoldScratch &f
     __syncwarp();
 }
 
-template <typename Get>
-__device__ void fold_node(const RoundBuffers &rb, const JobCounters &jc, const ApplyArgs &a,
-                          uint32_t node, uint32_t b, Get get, FoldScratch &fs) {
+// A node's counters as its fold starts, loaded before its entries are put in
+// order so that the loads overlap that work.
+struct NodeState {
+    double v;         // this lane's chain
+    uint32_t lu0;     // last_upd before the round
+    bool crossed;     // lane 25: approx reached 3 in an earlier round (top-k pass 1)
+};
+
+__device__ __forceinline__ NodeState fold_load(const JobCounters &jc, const ApplyArgs &a,
+                                               uint32_t node) {
     const int lane = threadIdx.x & 31;
-    const bool pass2 = a.pass == 2;
-    long long m = 0;
-    double acc = 0.0;
-    uint32_t lu = 0;
+    NodeState s{0.0, 0u, true};
     if (lane < kTrials) {
-        if (pass2) m = jc.mcrade[(uint64_t)node * kTrials + lane];
-    } else if (lane == 25) {
-        acc = jc.approx[node];
-        lu = jc.last_upd[node];
+        if (a.pass == 2) s.v = (double)jc.mcrade[(uint64_t)node * kTrials + lane];
     } else if (lane == 26) {
-        acc = jc.wimpy[node];
+        s.v = jc.wimpy[node];
+    } else {
+        s.v = jc.approx[node];
+        if (lane == 25) {
+            s.lu0 = jc.last_upd[node];
+            if (a.track_cross) s.crossed = jc.cross_flag[node] != 0;
+        }
     }
-    bool crossed = a.track_cross ? jc.cross_flag[node] != 0 : true;
+    return s;
+}
+
+// Folds the node's b entries; fill(r0) has lane i stage entry r0 + i (when
+// below b) in the scratch.
+template <typename Fill>
+__device__ void fold_node(const JobCounters &jc, const ApplyArgs &a, uint32_t node, uint32_t b,
+                          NodeState st, Fill fill, FoldScratch &fs) {
+    const int lane = threadIdx.x & 31;
+    const bool mc = lane < kTrials, wv = lane == 26;
+    double v = st.v;
+    uint32_t lu = 0;
     for (uint32_t r0 = 0; r0 < b; r0 += 32) {
-        const uint32_t r = r0 + lane;
-        if (r < b) {
-            const unsigned long long e = get(r);
-            const uint32_t sl = (uint32_t)(e >> 32);
-            const uint32_t c = (uint32_t)e;
-            fs.x[lane] = __dmul_rn((double)c, rb.inv_np[sl]);
-            fs.signs[lane] = pass2 ? rb.signs[sl] : 0u;
-            fs.sample[lane] = sl;
-        }
+        fill(r0);
         __syncwarp();
+        const bool pos = r0 + lane < b && fs.x[lane] > 0.;
+        const uint32_t pm = __ballot_sync(0xffffffffu, pos);
+        // 1 + global index of the last sample that adds to approx
+        if (pm) lu = a.first_sample + fs.sample[31 - __clz(pm)] + 1u;
         const uint32_t kmax = min(32u, b - r0);
-        if (lane < kTrials) {
-            if (pass2) {
-                // (int64)((double)m + s x) with m kept as an integer-valued
-                // double: the conversions to and from int64 are exact (|m| is
-                // at most the sample count, far below 2^53), so truncating in
-                // double gives the same value with one dependent step fewer
-                double md = (double)m;
-                for (uint32_t k = 0; k < kmax; k++) {
-                    const double x = fs.x[k];
-                    const bool plus = (fs.signs[k] >> lane) & 1u;
-                    md = trunc(__dadd_rn(md, plus ? x : -x));
-                }
-                m = (long long)md;
-            }
-        } else if (lane == 25) {
-            for (uint32_t k = 0; k < kmax; k++) {
-                const double x = fs.x[k];
-                if (x > 0.) {
-                    acc = __dadd_rn(acc, x);
-                    lu = a.first_sample + fs.sample[k] + 1u;
-                    if (!crossed && acc >= 3.0) {
-                        crossed = true;
-                        jc.cross_flag[node] = 1;
-                        const uint32_t q = atomicAdd(&jc.sc->n_cross, 1u);
-                        jc.cross_sample[q] = a.first_sample + fs.sample[k];
-                    }
-                }
-            }
-        } else if (lane == 26) {
-            for (uint32_t k = 0; k < kmax; k++) {
-                const double x = fs.x[k];
-                if (x > 0.) acc = __dadd_rn(acc, __dmul_rn(x, x));
-            }
+        int kc = -1;
+#pragma unroll 4
+        for (uint32_t k = 0; k < kmax; k++) {
+            const double x = fs.x[k];
+            const bool plus = (fs.signs[k] >> lane) & 1u;
+            // mcrade: (int64)((double)m + s x), m kept as an integer-valued
+            // double (|m| is at most the sample count, far below 2^53, so the
+            // conversions are exact and truncating in double is the same);
+            // approx and the wimpy variance add x and x * x when x > 0
+            const double add = x > 0. ? (wv ? __dmul_rn(x, x) : x) : 0.0;
+            const double y = mc ? (plus ? x : -x) : add;
+            const double t = __dadd_rn(v, y);
+            if (!st.crossed && kc < 0 && t >= 3.0) kc = (int)k;
+            v = mc ? trunc(t) : t;
+        }
+        if (kc >= 0) {  // lane 25 only: approx reached 3 at entry kc
+            st.crossed = true;
+            jc.cross_flag[node] = 1;
+            const uint32_t q = atomicAdd(&jc.sc->n_cross, 1u);
+            jc.cross_sample[q] = a.first_sample + fs.sample[kc];
         }
         __syncwarp();
     }
-    if (lane < kTrials) {
-        if (pass2) jc.mcrade[(uint64_t)node * kTrials + lane] = m;
+    if (mc) {
+        if (a.pass == 2) jc.mcrade[(uint64_t)node * kTrials + lane] = (long long)v;
     } else if (lane == 25) {
-        jc.approx[node] = acc;
+        jc.approx[node] = v;
         if (lu) {
-            if (jc.last_upd[node] == 0) fs.upd[fs.nupd++] = node;
+            if (st.lu0 == 0) fs.upd[fs.nupd++] = node;
             jc.last_upd[node] = lu;
         }
-        fs.sup_a = fmax(fs.sup_a, acc);
-    } else if (lane == 26) {
-        jc.wimpy[node] = acc;
-        fs.sup_w = fmax(fs.sup_w, acc);
+        fs.sup_a = fmax(fs.sup_a, v);
+    } else if (wv) {
+        jc.wimpy[node] = v;
+        fs.sup_w = fmax(fs.sup_w, v);
     }
     __syncwarp();
     if (fs.nupd == 32) upd_flush(jc, fs);
 }
 
-__device__ __forceinline__ void warp_bitonic_sort(unsigned long long &key) {
-    const int lane = threadIdx.x & 31;
-#pragma unroll
-    for (int k = 2; k <= 32; k <<= 1) {
-#pragma unroll
-        for (int j = k >> 1; j > 0; j >>= 1) {
-            const unsigned long long o = __shfl_xor_sync(0xffffffffu, key, j);
-            const bool take_min = ((lane & j) == 0) == ((lane & k) == 0);
-            key = take_min ? (key < o ? key : o) : (key > o ? key : o);
-        }
-    }
-}
-
-// Shared memory of the commit kernel: phase E's per-warp buffers and phase
-// F's sort buffer share one region.
-struct SmallSmem {
-    unsigned long long buf[kCommitThreads / 32][32];
+// Shared memory of phase D: the sub-round's per-sample factors (read by every
+// fold in place of global gathers), warp 0's large bucket in sample order, and
+// one fold scratch per warp.
+struct CommitSmem {
+    double s_inv[kLargeBucket];             // 1 / num_paths of the sub-round's samples
+    uint32_t s_sgn[kLargeBucket];           // their Rademacher signs (pass 2)
+    unsigned long long sbuf[kLargeBucket];  // warp 0's bucket, in sample order
+    uint32_t bits[kLargeBucket / 32];       // samples of that bucket
+    uint32_t wpre[kLargeBucket / 32];       // set bits before each word
     FoldScratch fsc[kCommitThreads / 32];
 };
-struct LargeSmem {
-    unsigned long long sbuf[kLargeBucket];
-    uint32_t bits[kLargeBucket / 32];  // samples of the bucket
-    uint32_t wpre[kLargeBucket / 32];  // set bits before each word
-    uint32_t wsum[32];
-    FoldScratch fsc;
-};
-constexpr size_t kCommitSmem = sizeof(LargeSmem) > sizeof(SmallSmem) ? sizeof(LargeSmem)
-                                                                        : sizeof(SmallSmem);
+constexpr size_t kCommitSmem = sizeof(CommitSmem);
+constexpr uint32_t kSmallWarps = kCommitThreads / 32 - 1;  // warps 1.. of each CTA
 
-// Buckets of at most 32 entries: one warp per node, eight touched nodes per
-// claim of the round's cursor (larger buckets are skipped: the CTA-wide fold
-// takes them).
+// Buckets of at most 32 entries, on warps 1.. of every CTA: touched node t
+// goes to warp t mod (CTAs x kSmallWarps), no cursor.  A bucket holds
+// distinct samples, so each entry's position in sample order is the number
+// of entries with a smaller sample (32 compares per lane, no sort).
 __device__ void apply_small(const RoundBuffers &rb, const JobCounters &jc, const ApplyArgs &a,
-                            uint32_t T, SmallSmem &sm) {
+                            uint32_t T, CommitSmem &sm) {
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    fold_begin(sm.fsc[wib]);
-    for (;;) {
-        uint32_t t0 = 0;
-        if (lane == 0) t0 = atomicAdd(rb.n_touched + 6, 8u);
-        t0 = __shfl_sync(0xffffffffu, t0, 0);
-        if (t0 >= T) break;
-        for (uint32_t t = t0; t < min(T, t0 + 8u); t++) {
-            const uint32_t b = rb.bucket_len[t];
-            if (b > 32) continue;
-            const uint32_t b0 = rb.bucket_off[t];
-            const uint32_t node = rb.touched[t];
-            unsigned long long key = (uint32_t)lane < b ? rb.entries[b0 + lane] : ~0ull;
-            warp_bitonic_sort(key);
-            sm.buf[wib][lane] = key;
-            __syncwarp();
-            fold_node(rb, jc, a, node, b, [&](uint32_t r) { return sm.buf[wib][r]; },
-                      sm.fsc[wib]);
-            __syncwarp();
-        }
+    FoldScratch &fs = sm.fsc[wib];
+    fold_begin(fs);
+    const uint32_t stride = gridDim.x * kSmallWarps;
+    for (uint32_t t = blockIdx.x * kSmallWarps + (uint32_t)(wib - 1); t < T; t += stride) {
+        const uint32_t b = __ldcg(&rb.bucket_len[t]);
+        if (b > 32) continue;
+        const uint32_t node = __ldcg(&rb.touched[t]);
+        const NodeState st = fold_load(jc, a, node);
+        const unsigned long long key =
+            (uint32_t)lane < b ? __ldcg(&rb.entries[__ldcg(&rb.bucket_off[t]) + lane]) : ~0ull;
+        uint32_t rank = 0;
+        for (uint32_t j = 0; j < b; j++) rank += __shfl_sync(0xffffffffu, key, (int)j) < key;
+        fold_node(jc, a, node, b, st,
+                  [&](uint32_t) {
+                      if ((uint32_t)lane < b) {
+                          const uint32_t sl = (uint32_t)(key >> 32);
+                          fs.x[rank] = __dmul_rn((double)(uint32_t)key, sm.s_inv[sl - a.lo]);
+                          fs.signs[rank] = sm.s_sgn[sl - a.lo];
+                          fs.sample[rank] = sl;
+                      }
+                  },
+                  fs);
     }
-    fold_flush(jc, sm.fsc[wib]);
+    fold_flush(jc, fs);
 }
 
-// Buckets of more than 32 entries: one CTA per node, claimed from a cursor.  The entries of a
-// bucket are distinct samples of the sub-round (a node is on a sample's path
-// map once), whose local index lies below kLargeBucket, so their order is
-// the rank of each sample in a bitmap of the sub-round: set one bit per
-// entry, prefix-count the bits per word, and each entry goes to its rank
-// (linear in the bucket; no comparison sort).
+// Buckets of more than 32 entries, on warp 0 of every CTA, claimed from a
+// cursor.  The entries of a bucket are distinct samples of the sub-round (a
+// node is on a sample's path map once), so their order is the rank of each
+// sample in a bitmap of the sub-round: set one bit per entry, prefix-count
+// the bits per word, and each entry goes to its rank (linear in the bucket;
+// no comparison sort).
 __device__ void apply_large(const RoundBuffers &rb, const JobCounters &jc, const ApplyArgs &a,
-                            LargeSmem &sm) {
+                            CommitSmem &sm) {
+    const int lane = threadIdx.x & 31;
+    FoldScratch &fs = sm.fsc[0];
+    fold_begin(fs);
     const uint32_t NL = __ldcg(rb.n_large);
-    unsigned long long *sbuf = sm.sbuf;
-    constexpr uint32_t kWords = kLargeBucket / 32;
-    __shared__ uint32_t claim;
-    if (threadIdx.x < 32) fold_begin(sm.fsc);
+    const uint32_t S = a.hi - a.lo;
+    const uint32_t nwords = (S + 31) / 32, per = (nwords + 31) / 32;
+    const uint32_t w0 = min(nwords, lane * per), w1 = min(nwords, w0 + per);
     for (;;) {
-        if (threadIdx.x == 0) claim = atomicAdd(rb.n_touched + 5, 1u);
-        __syncthreads();
-        const uint32_t li = claim;
-        __syncthreads();
+        uint32_t li = 0;
+        if (lane == 0) li = atomicAdd(rb.n_touched + 5, 1u);
+        li = __shfl_sync(0xffffffffu, li, 0);
         if (li >= NL) break;
         const uint32_t t = __ldcg(&rb.large[li]);
-        const uint32_t b0 = rb.bucket_off[t];
-        const uint32_t b = rb.bucket_len[t];
-        if (b > kLargeBucket) {
-            if (threadIdx.x == 0) atomicCAS(&jc.sc->error, 0, SILVAN_E_CAPACITY);
+        const uint32_t b0 = __ldcg(&rb.bucket_off[t]), b = __ldcg(&rb.bucket_len[t]);
+        if (b > S) {  // more entries than samples: not a bucket of distinct samples
+            if (lane == 0) atomicCAS(&jc.sc->error, 0, SILVAN_E_STATE);
             continue;
         }
-        for (uint32_t w = threadIdx.x; w < kWords; w += blockDim.x) sm.bits[w] = 0u;
-        __syncthreads();
-        for (uint32_t i = threadIdx.x; i < b; i += blockDim.x) {
-            const uint32_t sidx = (uint32_t)(rb.entries[b0 + i] >> 32) - a.lo;
-            if (sidx < kLargeBucket) atomicOr(&sm.bits[sidx >> 5], 1u << (sidx & 31));
+        const uint32_t node = __ldcg(&rb.touched[t]);
+        const NodeState st = fold_load(jc, a, node);
+        for (uint32_t w = w0; w < w1; w++) sm.bits[w] = 0u;
+        __syncwarp();
+        for (uint32_t i = lane; i < b; i += 32) {
+            const uint32_t sidx = (uint32_t)(__ldcg(&rb.entries[b0 + i]) >> 32) - a.lo;
+            if (sidx < S) atomicOr(&sm.bits[sidx >> 5], 1u << (sidx & 31));
             else atomicCAS(&jc.sc->error, 0, SILVAN_E_STATE);
         }
-        __syncthreads();
-        // exclusive prefix of the words' bit counts (one word per thread)
-        {
-            const uint32_t w = threadIdx.x;
-            const uint32_t c = w < kWords ? __popc(sm.bits[w]) : 0u;
-            uint32_t incl = c;
-            const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-            for (int o = 1; o < 32; o <<= 1) {
-                const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
-                if (lane >= o) incl += v;
-            }
-            if (lane == 31) sm.wsum[warp] = incl;
-            __syncthreads();
-            if (warp == 0) {
-                const uint32_t v = lane < (int)(blockDim.x >> 5) ? sm.wsum[lane] : 0u;
-                uint32_t vi = v;
-                for (int o = 1; o < 32; o <<= 1) {
-                    const uint32_t u = __shfl_up_sync(0xffffffffu, vi, o);
-                    if (lane >= o) vi += u;
-                }
-                sm.wsum[lane] = vi - v;
-            }
-            __syncthreads();
-            if (w < kWords) sm.wpre[w] = sm.wsum[warp] + incl - c;
+        __syncwarp();
+        // exclusive prefix of the words' bit counts (lane L owns words
+        // [L per, (L + 1) per))
+        uint32_t c = 0;
+        for (uint32_t w = w0; w < w1; w++) c += __popc(sm.bits[w]);
+        uint32_t incl = c;
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t u = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += u;
         }
-        __syncthreads();
-        for (uint32_t i = threadIdx.x; i < b; i += blockDim.x) {
-            const unsigned long long e = rb.entries[b0 + i];
+        uint32_t run = incl - c;
+        for (uint32_t w = w0; w < w1; w++) {
+            sm.wpre[w] = run;
+            run += __popc(sm.bits[w]);
+        }
+        __syncwarp();
+        for (uint32_t i = lane; i < b; i += 32) {
+            const unsigned long long e = __ldcg(&rb.entries[b0 + i]);
             const uint32_t sidx = (uint32_t)(e >> 32) - a.lo;
-            if (sidx < kLargeBucket) {
+            if (sidx < S) {
                 const uint32_t w = sidx >> 5;
-                sbuf[sm.wpre[w] + __popc(sm.bits[w] & ((1u << (sidx & 31)) - 1u))] = e;
+                sm.sbuf[sm.wpre[w] + __popc(sm.bits[w] & ((1u << (sidx & 31)) - 1u))] = e;
             }
         }
-        __syncthreads();
-        if (threadIdx.x < 32) {
-            const uint32_t node = rb.touched[t];
-            fold_node(rb, jc, a, node, b, [&](uint32_t r) { return sbuf[r]; }, sm.fsc);
-        }
-        __syncthreads();
+        __syncwarp();
+        fold_node(jc, a, node, b, st,
+                  [&](uint32_t r0) {
+                      const uint32_t r = r0 + lane;
+                      if (r < b) {
+                          const unsigned long long e = sm.sbuf[r];
+                          const uint32_t sl = (uint32_t)(e >> 32);
+                          fs.x[lane] = __dmul_rn((double)(uint32_t)e, sm.s_inv[sl - a.lo]);
+                          fs.signs[lane] = sm.s_sgn[sl - a.lo];
+                          fs.sample[lane] = sl;
+                      }
+                  },
+                  fs);
     }
-    if (threadIdx.x < 32) fold_flush(jc, sm.fsc);
+    fold_flush(jc, fs);
 }
 
 __device__ void commit_sums(const RoundBuffers &rb, const JobCounters &jc, const ApplyArgs &a) {
@@ -499,12 +491,17 @@ __global__ void __launch_bounds__(kCommitThreads, 1) commit_round_kernel(const A
         if (!grid_barrier(bar)) goto timeout;
         bucket_scatter(rb, a);
         if (!grid_barrier(bar)) goto timeout;
-        // the large buckets first (CTA-wide, few), then the small ones
-        // (one warp each): the CTAs without a large bucket start on the
-        // small ones at once
-        apply_large(rb, jc, a, *reinterpret_cast<LargeSmem *>(commit_smem));
+        CommitSmem &sm = *reinterpret_cast<CommitSmem *>(commit_smem);
+        // the sub-round's factors into shared memory, then warp 0 folds the
+        // large buckets while the other warps fold the small ones
+        for (uint32_t i = threadIdx.x; i < a.hi - a.lo; i += blockDim.x) {
+            sm.s_inv[i] = __ldcg(&rb.inv_np[a.lo + i]);
+            sm.s_sgn[i] = a.pass == 2 ? __ldcg(&rb.signs[a.lo + i]) : 0u;
+        }
         __syncthreads();
-        apply_small(rb, jc, a, T, *reinterpret_cast<SmallSmem *>(commit_smem));
+        if (threadIdx.x < 32) apply_large(rb, jc, a, sm);
+        else apply_small(rb, jc, a, T, sm);
+        __syncthreads();
         commit_sums(rb, jc, a);
         // the scatter cursors back to zero for the next round
         for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < T;

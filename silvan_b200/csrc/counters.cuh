@@ -10,7 +10,7 @@
 
 namespace silvan {
 
-constexpr uint32_t kLargeBucket = 16384;  // samples per apply sub-round (bucket bound)
+constexpr uint32_t kLargeBucket = 8192;  // samples per apply sub-round (bucket bound)
 constexpr int kMaxPartitions = 128;
 
 // Job-level scalars kept on the device.
@@ -49,11 +49,11 @@ struct RoundBuffers {
     uint32_t *touched;       // distinct nodes of the round
     // control words of a commit round, zeroed before it: [0] touched nodes,
     // [1] large buckets, [2..3] grid barrier, [4] bucket-space cursor,
-    // [5] large-bucket claims, [6] small-bucket claims, [7] unused
+    // [5] large-bucket claims, [6..7] unused
     uint32_t *n_touched;
     uint32_t *bucket_off;    // start of each touched node's bucket
     uint32_t *bucket_len;    // its number of entries
-    uint32_t *large;         // buckets of more than 32 entries (listed by apply_small)
+    uint32_t *large;         // buckets of more than 32 entries (listed by bucket_alloc)
     uint32_t *n_large;       // = n_touched + 1 (both zeroed together)
     unsigned long long *entries;  // sample << 32 | count, grouped by node
     uint32_t *work_counter;  // sampler work counter
