@@ -15,6 +15,7 @@
 // node.
 #include <algorithm>
 #include <cfloat>
+#include <climits>
 #include <cstring>
 #include <vector>
 
@@ -227,19 +228,29 @@ struct NodeState {
     bool crossed;     // lane 25: approx reached 3 in an earlier round (top-k pass 1)
 };
 
-__device__ __forceinline__ NodeState fold_load(const JobCounters &jc, const ApplyArgs &a,
-                                               uint32_t node) {
+// A journaled round also saves them at the node's touched position t.
+__device__ __forceinline__ NodeState fold_load(const JobCounters &jc, const RoundJournal &jr,
+                                               const ApplyArgs &a, uint32_t node, uint32_t t) {
     const int lane = threadIdx.x & 31;
     NodeState s{0.0, 0u, true};
     if (lane < kTrials) {
-        if (a.pass == 2) s.v = (double)jc.mcrade[(uint64_t)node * kTrials + lane];
+        if (a.pass == 2) {
+            const long long m = jc.mcrade[(uint64_t)node * kTrials + lane];
+            if (a.journal) jr.mcrade[(uint64_t)t * kTrials + lane] = m;
+            s.v = (double)m;
+        }
     } else if (lane == 26) {
         s.v = jc.wimpy[node];
+        if (a.journal) jr.wimpy[t] = s.v;
     } else {
         s.v = jc.approx[node];
         if (lane == 25) {
             s.lu0 = jc.last_upd[node];
             if (a.track_cross) s.crossed = jc.cross_flag[node] != 0;
+            if (a.journal) {
+                jr.approx[t] = s.v;
+                jr.last_upd[t] = s.lu0;
+            }
         }
     }
     return s;
@@ -320,8 +331,8 @@ constexpr uint32_t kSmallWarps = kCommitThreads / 32 - 1;  // warps 1.. of each 
 // goes to warp t mod (CTAs x kSmallWarps), no cursor.  A bucket holds
 // distinct samples, so each entry's position in sample order is the number
 // of entries with a smaller sample (32 compares per lane, no sort).
-__device__ void apply_small(const RoundBuffers &rb, const JobCounters &jc, const ApplyArgs &a,
-                            uint32_t T, CommitSmem &sm) {
+__device__ void apply_small(const RoundBuffers &rb, const JobCounters &jc, const RoundJournal &jr,
+                            const ApplyArgs &a, uint32_t T, CommitSmem &sm) {
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     FoldScratch &fs = sm.fsc[wib];
     fold_begin(fs);
@@ -330,7 +341,7 @@ __device__ void apply_small(const RoundBuffers &rb, const JobCounters &jc, const
         const uint32_t b = __ldcg(&rb.bucket_len[t]);
         if (b > 32) continue;
         const uint32_t node = __ldcg(&rb.touched[t]);
-        const NodeState st = fold_load(jc, a, node);
+        const NodeState st = fold_load(jc, jr, a, node, t);
         const unsigned long long key =
             (uint32_t)lane < b ? __ldcg(&rb.entries[__ldcg(&rb.bucket_off[t]) + lane]) : ~0ull;
         uint32_t rank = 0;
@@ -355,8 +366,8 @@ __device__ void apply_small(const RoundBuffers &rb, const JobCounters &jc, const
 // sample in a bitmap of the sub-round: set one bit per entry, prefix-count
 // the bits per word, and each entry goes to its rank (linear in the bucket;
 // no comparison sort).
-__device__ void apply_large(const RoundBuffers &rb, const JobCounters &jc, const ApplyArgs &a,
-                            CommitSmem &sm) {
+__device__ void apply_large(const RoundBuffers &rb, const JobCounters &jc, const RoundJournal &jr,
+                            const ApplyArgs &a, CommitSmem &sm) {
     const int lane = threadIdx.x & 31;
     FoldScratch &fs = sm.fsc[0];
     fold_begin(fs);
@@ -376,7 +387,7 @@ __device__ void apply_large(const RoundBuffers &rb, const JobCounters &jc, const
             continue;
         }
         const uint32_t node = __ldcg(&rb.touched[t]);
-        const NodeState st = fold_load(jc, a, node);
+        const NodeState st = fold_load(jc, jr, a, node, t);
         for (uint32_t w = w0; w < w1; w++) sm.bits[w] = 0u;
         __syncwarp();
         for (uint32_t i = lane; i < b; i += 32) {
@@ -476,17 +487,43 @@ __device__ void commit_sums(const RoundBuffers &rb, const JobCounters &jc, const
 }
 
 
-__global__ void __launch_bounds__(kCommitThreads, 1) commit_round_kernel(const ApplyState *st) {
+// The last CTA out zeroes the round's control words for the next round
+// (word 7, the touched count, stays for undo_round).
+__device__ void commit_exit(const RoundBuffers &rb) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(rb.n_touched + 6, 1u) == gridDim.x - 1) {
+            rb.n_touched[0] = 0u;
+            rb.n_touched[1] = 0u;
+            rb.n_touched[4] = 0u;
+            rb.n_touched[5] = 0u;
+            rb.n_touched[6] = 0u;
+            __threadfence();
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kCommitThreads, 1) commit_round_kernel(const ApplyState st) {
     extern __shared__ __align__(16) unsigned char commit_smem[];
-    __shared__ uint32_t tmp[34];
-    const RoundBuffers rb = st->rb;
-    const JobCounters jc = st->jc;
-    const ApplyArgs a = st->a;
+    const RoundBuffers &rb = st.rb;
+    const JobCounters &jc = st.jc;
+    const RoundJournal &jr = st.jr;
+    const ApplyArgs &a = st.a;
     uint32_t *bar = rb.n_touched + 2;
+    if (a.journal && blockIdx.x == 0) {
+        // the scalars and path-length counts as the round starts (phase D
+        // is the first to change them)
+        const unsigned long long *src = reinterpret_cast<const unsigned long long *>(jc.sc);
+        unsigned long long *dst = reinterpret_cast<unsigned long long *>(jr.sc);
+        for (uint32_t i = threadIdx.x; i < sizeof(JobScalars) / 8; i += blockDim.x) dst[i] = src[i];
+        for (uint32_t i = threadIdx.x; i <= a.D; i += blockDim.x) jr.sp_lengths[i] = jc.sp_lengths[i];
+    }
     bucket_count(rb, a);
     if (!grid_barrier(bar)) goto timeout;
     {
         const uint32_t T = __ldcg(rb.n_touched);
+        if (blockIdx.x == 0 && threadIdx.x == 0) rb.n_touched[7] = T;
         bucket_alloc(rb, T);
         if (!grid_barrier(bar)) goto timeout;
         bucket_scatter(rb, a);
@@ -499,8 +536,8 @@ __global__ void __launch_bounds__(kCommitThreads, 1) commit_round_kernel(const A
             sm.s_sgn[i] = a.pass == 2 ? __ldcg(&rb.signs[a.lo + i]) : 0u;
         }
         __syncthreads();
-        if (threadIdx.x < 32) apply_large(rb, jc, a, sm);
-        else apply_small(rb, jc, a, T, sm);
+        if (threadIdx.x < 32) apply_large(rb, jc, jr, a, sm);
+        else apply_small(rb, jc, jr, a, T, sm);
         __syncthreads();
         commit_sums(rb, jc, a);
         // the scatter cursors back to zero for the next round
@@ -508,9 +545,11 @@ __global__ void __launch_bounds__(kCommitThreads, 1) commit_round_kernel(const A
              t += gridDim.x * blockDim.x)
             rb.node_cnt[rb.touched[t]] = 0;
     }
+    commit_exit(rb);
     return;
 timeout:
     if (threadIdx.x == 0) atomicCAS(&jc.sc->error, 0, SILVAN_E_TIMEOUT);
+    commit_exit(rb);
 }
 
 int g_commit_grid = 0;  // resident CTAs of commit_round_kernel (apply_init)
@@ -534,11 +573,34 @@ cudaError_t apply_init() {
     return cudaSuccess;
 }
 
-cudaError_t apply_round(const ApplyState *st, uint32_t *n_touched, cudaStream_t stream) {
+// One warp per node of the round's touched list, lanes as in the fold.
+__global__ void undo_round_kernel(RoundBuffers rb, JobCounters jc, RoundJournal jr, int pass,
+                                  uint32_t D) {
+    const uint32_t T = __ldcg(rb.n_touched + 7);
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < T; t += nw) {
+        const uint32_t node = rb.touched[t];
+        if (lane < kTrials) {
+            if (pass == 2)
+                jc.mcrade[(uint64_t)node * kTrials + lane] = jr.mcrade[(uint64_t)t * kTrials + lane];
+        } else if (lane == 25) {
+            jc.approx[node] = jr.approx[t];
+            jc.last_upd[node] = jr.last_upd[t];
+        } else if (lane == 26) {
+            jc.wimpy[node] = jr.wimpy[t];
+        }
+    }
+    if (blockIdx.x == 0) {
+        const unsigned long long *src = reinterpret_cast<const unsigned long long *>(jr.sc);
+        unsigned long long *dst = reinterpret_cast<unsigned long long *>(jc.sc);
+        for (uint32_t i = threadIdx.x; i < sizeof(JobScalars) / 8; i += blockDim.x) dst[i] = src[i];
+        for (uint32_t i = threadIdx.x; i <= D; i += blockDim.x) jc.sp_lengths[i] = jr.sp_lengths[i];
+    }
+}
+
+cudaError_t apply_round(const ApplyState &st, cudaStream_t stream) {
     if (g_commit_grid <= 0) return cudaErrorNotReady;
-    // the round's control words (see RoundBuffers::n_touched)
-    cudaError_t e = cudaMemsetAsync(n_touched, 0, 8 * sizeof(uint32_t), stream);
-    if (e != cudaSuccess) return e;
     cudaLaunchConfig_t cfg{};
     cfg.gridDim = dim3((unsigned)g_commit_grid);
     cfg.blockDim = dim3(kCommitThreads);
@@ -554,26 +616,33 @@ cudaError_t apply_round(const ApplyState *st, uint32_t *n_touched, cudaStream_t 
 
 namespace {
 
-__global__ void stop_init_kernel(StopReduction *out, int nparts, long long init) {
-    for (int i = threadIdx.x; i < nparts * kTrials; i += blockDim.x) out->mc_max[i] = init;
-    for (int i = threadIdx.x; i < nparts; i += blockDim.x) {
-        out->wimpy_max[i] = 0.0;
-        out->touched[i] = 0;
+// Neutral accumulator: every maximum at its identity.
+__global__ void stop_init_kernel(StopReduction *acc) {
+    for (int i = threadIdx.x; i < kMaxPartitions * kTrials; i += blockDim.x)
+        acc->mc_max[i] = LLONG_MIN;
+    for (int i = threadIdx.x; i < kMaxPartitions; i += blockDim.x) {
+        acc->wimpy_max[i] = 0.0;
+        acc->touched[i] = 0;
     }
     if (threadIdx.x == 0) {
-        out->approx_max = 0.0;
-        out->wimpy_all_max = 0.0;
+        acc->approx_max = 0.0;
+        acc->wimpy_all_max = 0.0;
     }
 }
 
 // One warp per updated node: lanes 0..24 read the node's 25 trials (one
-// 200-byte row), lane 25 approx and wimpy.
-__global__ void __launch_bounds__(512) stop_reduce_kernel(JobCounters jc, int nparts,
-                                                          long long init, StopReduction *out) {
+// 200-byte row), lane 25 approx and wimpy.  Each CTA folds its nodes in
+// shared memory and into the device accumulator; the last CTA out writes the
+// result, the job's scalars and the path-length counts to the (host-mapped)
+// readback and leaves the accumulator neutral for the next check.
+__global__ void __launch_bounds__(512) stop_reduce_kernel(JobCounters jc, int nparts, uint32_t D,
+                                                          StopReduction *acc, uint32_t *ticket,
+                                                          StopReadback rb) {
     __shared__ long long smc[kMaxPartitions * kTrials];
     __shared__ unsigned long long sw[kMaxPartitions];
     __shared__ uint32_t st[kMaxPartitions];
-    for (int i = threadIdx.x; i < nparts * kTrials; i += blockDim.x) smc[i] = init;
+    __shared__ bool last;
+    for (int i = threadIdx.x; i < nparts * kTrials; i += blockDim.x) smc[i] = LLONG_MIN;
     for (int i = threadIdx.x; i < nparts; i += blockDim.x) {
         sw[i] = 0ull;
         st[i] = 0;
@@ -605,33 +674,130 @@ __global__ void __launch_bounds__(512) stop_reduce_kernel(JobCounters jc, int np
         wmax = y > wmax ? y : wmax;
     }
     if (lane == 0) {
-        if (amax) atomicMax(reinterpret_cast<unsigned long long *>(&out->approx_max), amax);
-        if (wmax) atomicMax(reinterpret_cast<unsigned long long *>(&out->wimpy_all_max), wmax);
+        if (amax) atomicMax(reinterpret_cast<unsigned long long *>(&acc->approx_max), amax);
+        if (wmax) atomicMax(reinterpret_cast<unsigned long long *>(&acc->wimpy_all_max), wmax);
     }
     __syncthreads();
     for (int i = threadIdx.x; i < nparts * kTrials; i += blockDim.x)
-        if (smc[i] != init) atomicMax(&out->mc_max[i], smc[i]);
+        if (smc[i] != LLONG_MIN) atomicMax(&acc->mc_max[i], smc[i]);
     for (int i = threadIdx.x; i < nparts; i += blockDim.x) {
-        if (sw[i]) atomicMax(reinterpret_cast<unsigned long long *>(&out->wimpy_max[i]), sw[i]);
-        if (st[i]) atomicAdd(&out->touched[i], st[i]);
+        if (sw[i]) atomicMax(reinterpret_cast<unsigned long long *>(&acc->wimpy_max[i]), sw[i]);
+        if (st[i]) atomicAdd(&acc->touched[i], st[i]);
     }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    for (int i = threadIdx.x; i < nparts * kTrials; i += blockDim.x) {
+        rb.red->mc_max[i] = __ldcg(&acc->mc_max[i]);
+        acc->mc_max[i] = LLONG_MIN;
+    }
+    for (int i = threadIdx.x; i < nparts; i += blockDim.x) {
+        rb.red->wimpy_max[i] = __ldcg(&acc->wimpy_max[i]);
+        rb.red->touched[i] = __ldcg(&acc->touched[i]);
+        acc->wimpy_max[i] = 0.0;
+        acc->touched[i] = 0;
+    }
+    if (threadIdx.x == 0) {
+        rb.red->approx_max = __ldcg(&acc->approx_max);
+        rb.red->wimpy_all_max = __ldcg(&acc->wimpy_all_max);
+        acc->approx_max = 0.0;
+        acc->wimpy_all_max = 0.0;
+        *ticket = 0u;
+    }
+    const unsigned long long *src = reinterpret_cast<const unsigned long long *>(jc.sc);
+    unsigned long long *dst = reinterpret_cast<unsigned long long *>(rb.sc);
+    for (uint32_t i = threadIdx.x; i < sizeof(JobScalars) / 8; i += blockDim.x) dst[i] = __ldcg(&src[i]);
+    if (rb.sp)
+        for (uint32_t i = threadIdx.x; i <= D; i += blockDim.x) rb.sp[i] = __ldcg(&jc.sp_lengths[i]);
+}
+
+// Peeling index of node v (Probabilistic.cpp:855-862), stored in peel_idx.
+// The C library's log may differ from the device's by an ulp; the nodes
+// where that could move (int)t are listed so that the host recomputes them.
+__device__ __forceinline__ int32_t peel_index_of(const JobCounters &jc, uint32_t v, double m,
+                                                 double la, uint32_t *unc, uint32_t *n_unc,
+                                                 uint32_t cap) {
+    const double ew = jc.wimpy[v] / m;
+    const double mi = fmin(1. / ew, m);
+    const double t = log(mi) / la + 1;
+    const int32_t idx = (int)t;
+    jc.peel_idx[v] = idx;
+    const double fr = t - floor(t);
+    if (fr < 1e-9 || fr > 1.0 - 1e-9) {
+        uint32_t k = atomicAdd(n_unc, 1u);
+        if (k < cap) unc[k] = v;
+    }
+    return idx;
 }
 
 __global__ void peel_index_kernel(JobCounters jc, uint32_t n, double m, double a, uint32_t *unc,
                                   uint32_t *n_unc, uint32_t cap) {
     const double la = log(a);
-    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
-        const double ew = jc.wimpy[v] / m;
-        const double mi = fmin(1. / ew, m);
-        const double t = log(mi) / la + 1;
-        jc.peel_idx[v] = (int)t;
-        // the C library's log may differ from the device's by an ulp; flag the
-        // nodes where that could move (int)t so the host recomputes them
-        const double fr = t - floor(t);
-        if (fr < 1e-9 || fr > 1.0 - 1e-9) {
-            uint32_t k = atomicAdd(n_unc, 1u);
-            if (k < cap) unc[k] = v;
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x)
+        peel_index_of(jc, v, m, la, unc, n_unc, cap);
+}
+
+// The end of pass 1 in one kernel: with peeling (nbins > 0) every node's
+// index, the uncertain list and the histogram of the indices over
+// [idx_min, idx_min + nbins) (hist and n_unc zeroed before); the last CTA
+// out copies the histogram, the uncertain count, the scalars and the
+// path-length counts to `out` (host-mapped).
+__global__ void __launch_bounds__(512) pass1_readback_kernel(
+    JobCounters jc, uint32_t n, double m, double a, int32_t idx_min, int32_t nbins,
+    uint32_t *hist, uint32_t *unc, uint32_t *n_unc, uint32_t cap, uint32_t D, uint32_t *ticket,
+    Pass1Readback out) {
+    extern __shared__ uint32_t sh[];
+    __shared__ bool last;
+    const bool local = nbins > 0 && nbins <= kPeelLocalBins;
+    if (local)
+        for (int i = threadIdx.x; i < nbins; i += blockDim.x) sh[i] = 0;
+    __syncthreads();
+    if (nbins > 0) {
+        const double la = log(a);
+        for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n;
+             v += gridDim.x * blockDim.x) {
+            int32_t b = peel_index_of(jc, v, m, la, unc, n_unc, cap) - idx_min;
+            b = b < 0 ? 0 : (b >= nbins ? nbins - 1 : b);
+            atomicAdd(local ? &sh[b] : &hist[b], 1u);
         }
+    }
+    __syncthreads();
+    if (local)
+        for (int i = threadIdx.x; i < nbins; i += blockDim.x)
+            if (sh[i]) atomicAdd(&hist[i], sh[i]);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    for (int i = threadIdx.x; i < nbins; i += blockDim.x) out.hist[i] = __ldcg(&hist[i]);
+    if (threadIdx.x == 0) {
+        *out.n_unc = __ldcg(n_unc);
+        *ticket = 0u;
+    }
+    const unsigned long long *src = reinterpret_cast<const unsigned long long *>(jc.sc);
+    unsigned long long *dst = reinterpret_cast<unsigned long long *>(out.sc);
+    for (uint32_t i = threadIdx.x; i < sizeof(JobScalars) / 8; i += blockDim.x) dst[i] = __ldcg(&src[i]);
+    for (uint32_t i = threadIdx.x; i <= D; i += blockDim.x) out.sp[i] = __ldcg(&jc.sp_lengths[i]);
+}
+
+// Zeroes approx, wimpy and last_upd of the nodes on upd_list (every node
+// with a non-zero one): the counters of pass 2 start from zero.
+__global__ void reset_updated_kernel(JobCounters jc) {
+    const uint32_t T = jc.sc->n_upd;
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < T; t += gridDim.x * blockDim.x) {
+        const uint32_t v = jc.upd_list[t];
+        jc.approx[v] = 0.0;
+        jc.wimpy[v] = 0.0;
+        jc.last_upd[v] = 0u;
     }
 }
 
@@ -676,16 +842,28 @@ __global__ void divide_kernel(const double *approx, double m, double *out, uint3
         out[v] = __ddiv_rn(approx[v], m);
 }
 
+cudaError_t undo_round(const RoundBuffers &rb, const JobCounters &jc, const RoundJournal &jr,
+                       int pass, uint32_t D, cudaStream_t stream) {
+    undo_round_kernel<<<296, 512, 0, stream>>>(rb, jc, jr, pass, D);
+    return cudaGetLastError();
+}
+
 cudaError_t divide_estimates(const double *approx, double num_samples, double *out, uint32_t n,
                              cudaStream_t stream) {
     divide_kernel<<<592, 256, 0, stream>>>(approx, num_samples, out, n);
     return cudaGetLastError();
 }
 
-cudaError_t stop_reduce(const JobCounters &jc, int nparts, long long init,
-                        StopReduction *out_dev, cudaStream_t stream) {
-    stop_init_kernel<<<1, 256, 0, stream>>>(out_dev, nparts, init);
-    stop_reduce_kernel<<<296, 512, 0, stream>>>(jc, nparts, init, out_dev);
+cudaError_t stop_reduce_init(StopReduction *acc, uint32_t *ticket, cudaStream_t stream) {
+    stop_init_kernel<<<1, 256, 0, stream>>>(acc);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    return cudaMemsetAsync(ticket, 0, sizeof(uint32_t), stream);
+}
+
+cudaError_t stop_reduce(const JobCounters &jc, int nparts, uint32_t D, StopReduction *acc,
+                        uint32_t *ticket, const StopReadback &out, cudaStream_t stream) {
+    stop_reduce_kernel<<<296, 512, 0, stream>>>(jc, nparts, D, acc, ticket, out);
     return cudaGetLastError();
 }
 
@@ -697,10 +875,29 @@ cudaError_t peel_index(const JobCounters &jc, uint32_t n, double num_samples, do
     return cudaGetLastError();
 }
 
+cudaError_t pass1_readback(const JobCounters &jc, uint32_t n, double num_samples, double a,
+                           int32_t idx_min, int32_t nbins, uint32_t *hist, uint32_t *uncertain,
+                           uint32_t *n_uncertain, uint32_t cap, uint32_t D, uint32_t *ticket,
+                           const Pass1Readback &out, cudaStream_t stream) {
+    cudaError_t e = cudaMemsetAsync(n_uncertain, 0, sizeof(uint32_t), stream);
+    if (e == cudaSuccess && nbins > 0)
+        e = cudaMemsetAsync(hist, 0, sizeof(uint32_t) * nbins, stream);
+    if (e != cudaSuccess) return e;
+    const size_t smem = nbins > 0 && nbins <= kPeelLocalBins ? sizeof(uint32_t) * nbins : 0;
+    pass1_readback_kernel<<<296, 512, smem, stream>>>(jc, n, num_samples, a, idx_min, nbins, hist,
+                                                      uncertain, n_uncertain, cap, D, ticket, out);
+    return cudaGetLastError();
+}
+
+cudaError_t reset_updated(const JobCounters &jc, cudaStream_t stream) {
+    reset_updated_kernel<<<296, 512, 0, stream>>>(jc);
+    return cudaGetLastError();
+}
+
 cudaError_t peel_hist(const JobCounters &jc, uint32_t n, int32_t idx_min, int32_t nbins,
                       uint32_t *hist, cudaStream_t stream) {
     cudaMemsetAsync(hist, 0, sizeof(uint32_t) * nbins, stream);
-    if (nbins <= 8192)
+    if (nbins <= kPeelLocalBins)
         peel_hist_kernel<<<296, 512, sizeof(uint32_t) * nbins, stream>>>(jc, n, idx_min, nbins,
                                                                           hist);
     else

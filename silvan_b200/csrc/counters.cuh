@@ -29,6 +29,8 @@ struct JobScalars {
     uint32_t pad;
 };
 
+static_assert(sizeof(JobScalars) % 8 == 0, "JobScalars is copied in 8-byte words");
+
 struct RoundBuffers {
     // per round-local sample
     int32_t *pl;
@@ -47,9 +49,10 @@ struct RoundBuffers {
     // bucketing by node
     uint32_t *node_cnt;      // n, zero between rounds
     uint32_t *touched;       // distinct nodes of the round
-    // control words of a commit round, zeroed before it: [0] touched nodes,
-    // [1] large buckets, [2..3] grid barrier, [4] bucket-space cursor,
-    // [5] large-bucket claims, [6..7] unused
+    // control words of the commit rounds (zero when allocated; each round
+    // leaves them as it found them): [0] touched nodes, [1] large buckets,
+    // [2..3] grid barrier, [4] bucket-space cursor, [5] large-bucket claims,
+    // [6] CTAs done; [7] touched nodes of the last round (read by undo_round)
     uint32_t *n_touched;
     uint32_t *bucket_off;    // start of each touched node's bucket
     uint32_t *bucket_len;    // its number of entries
@@ -82,33 +85,51 @@ struct ApplyArgs {
     int32_t pass;            // 1 or 2 (pass 2 updates mcrade)
     int32_t track_cross;     // pass 1 of top-k mode
     uint32_t D;
+    int32_t journal;         // save what the round changes (RoundJournal) so it can be undone
 };
 
-// Device-resident copies of the three structs above, so that the apply
-// pipeline can be captured once in a CUDA graph and replayed every round.
+// What a journaled commit round overwrites: the old counters of each node it
+// folds (indexed by the node's position on the round's touched list), the
+// job's scalars and the shortest-path length counts.  undo_round puts them
+// back, which leaves the counters as they were before the round.  Sized for
+// every node of the graph (a round touches each node at most once).
+struct RoundJournal {
+    long long *mcrade;     // n x 25 (pass 2 only)
+    double *approx;        // n
+    double *wimpy;         // n
+    uint32_t *last_upd;    // n
+    JobScalars *sc;        // 1
+    uint64_t *sp_lengths;  // D + 1
+};
+
+// Everything a commit round reads, passed to its kernel by value.
 struct ApplyState {
     RoundBuffers rb;
     JobCounters jc;
+    RoundJournal jr;
     ApplyArgs a;
 };
 
-// Kernels apply_round launches: one cooperative kernel (after a memset).
+// Kernels apply_round launches: one cooperative kernel.
 constexpr int kApplyRoundKernels = 1;
 
 // Commits round-local samples [a.lo, a.hi) of the round buffers to the job
-// counters, all read from `st` on the device: one cooperative kernel whose
-// phases are separated by grid-wide barriers.  Launches only, with a fixed
-// grid, so it can be captured in a CUDA graph.  n_touched is the RoundBuffers
-// field of the same struct (its eight control words are zeroed here before
-// the kernel).
-cudaError_t apply_round(const ApplyState *st, uint32_t *n_touched, cudaStream_t stream);
+// counters: one cooperative kernel whose phases are separated by grid-wide
+// barriers, with st as its argument.
+cudaError_t apply_round(const ApplyState &st, cudaStream_t stream);
 // Function attributes and resident grid of the commit kernel on the current
 // device (call before capturing).
 cudaError_t apply_init();
+// Restores what the last commit round (journaled, and the last round on
+// rb) changed: the nodes of rb's touched list, the scalars, the path-length
+// counts.
+cudaError_t undo_round(const RoundBuffers &rb, const JobCounters &jc, const RoundJournal &jr,
+                       int pass, uint32_t D, cudaStream_t stream);
 
 // Reduction for one stopping-rule evaluation: per partition and trial the
-// maximum of mcrade (initialised to -n_pairs), per partition the maximum of
-// emp_wimpy_vars, and the global maxima of approx and emp_wimpy_vars.
+// maximum of mcrade (LLONG_MIN when no node of the partition was updated;
+// the host takes the larger of it and -n_pairs), per partition the maximum
+// of emp_wimpy_vars, and the global maxima of approx and emp_wimpy_vars.
 // Only the nodes on upd_list are read: every other node still has
 // approx = wimpy = mcrade = 0, which the host folds in per partition from
 // touched[] (a partition with fewer touched nodes than members has zeros).
@@ -123,8 +144,21 @@ struct StopReduction {
 cudaError_t divide_estimates(const double *approx, double num_samples, double *out, uint32_t n,
                              cudaStream_t stream);
 
-cudaError_t stop_reduce(const JobCounters &jc, int nparts, long long init,
-                        StopReduction *out_dev, cudaStream_t stream);
+// Where a check's results land (host-mapped memory, read after the kernel):
+// the reduction, the job's scalars, the D + 1 path-length counts (sp may be
+// null).
+struct StopReadback {
+    StopReduction *red;
+    JobScalars *sc;
+    uint64_t *sp;
+};
+// The device accumulator of stop_reduce and its CTA ticket, made neutral once
+// (stop_reduce leaves them neutral).
+cudaError_t stop_reduce_init(StopReduction *acc, uint32_t *ticket, cudaStream_t stream);
+// One kernel: the reduction over upd_list plus the scalars and path-length
+// counts, written to `out`.
+cudaError_t stop_reduce(const JobCounters &jc, int nparts, uint32_t D, StopReduction *acc,
+                        uint32_t *ticket, const StopReadback &out, cudaStream_t stream);
 
 // Empirical peeling index of every node (Probabilistic.cpp:855-862), with the
 // nodes whose index is within rounding distance of a boundary listed so that
@@ -136,6 +170,25 @@ cudaError_t peel_map(const JobCounters &jc, uint32_t n, const int32_t *lut, int3
                      int32_t lut_size, uint32_t *hist, cudaStream_t stream);
 cudaError_t peel_hist(const JobCounters &jc, uint32_t n, int32_t idx_min, int32_t nbins,
                       uint32_t *hist, cudaStream_t stream);
+constexpr int32_t kPeelLocalBins = 8192;  // histograms up to this size are built in shared memory
+
+// Where the end-of-pass-1 read lands (host-mapped memory).
+struct Pass1Readback {
+    JobScalars *sc;
+    uint64_t *sp;      // D + 1 path-length counts
+    uint32_t *hist;    // nbins peeling-index counts
+    uint32_t *n_unc;   // uncertain indices listed
+};
+// One kernel: peel_index and peel_hist when nbins > 0 (hist and n_uncertain
+// are zeroed here), then the histogram, the uncertain count, the scalars and
+// the path-length counts copied to `out`.  ticket is a zero word that the
+// kernel leaves zero.
+cudaError_t pass1_readback(const JobCounters &jc, uint32_t n, double num_samples, double a,
+                           int32_t idx_min, int32_t nbins, uint32_t *hist, uint32_t *uncertain,
+                           uint32_t *n_uncertain, uint32_t cap, uint32_t D, uint32_t *ticket,
+                           const Pass1Readback &out, cudaStream_t stream);
+// approx, wimpy and last_upd back to zero on the nodes of upd_list.
+cudaError_t reset_updated(const JobCounters &jc, cudaStream_t stream);
 
 // Ranking of the top-k mode (the reference's Ranking_list,
 // silvan/src/Ranking_list.cpp:20-43, as Probabilistic.cpp:587-687 reads it):

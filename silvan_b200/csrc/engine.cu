@@ -34,7 +34,6 @@ constexpr uint32_t kRoundSamples = 65536;  // samples per job per round
 constexpr uint64_t kInitialRecords = 1u << 20;
 constexpr uint32_t kBlock = 11;  // samples per block (Probabilistic.cpp:829,1061)
 constexpr uint32_t kUncertainCap = 1u << 16;
-constexpr uint32_t kArgRing = 64;
 
 // Caching allocator for device and pinned host memory.  Requests start and
 // finish all the time in a serving process, and cudaMalloc / cudaFree (and
@@ -907,7 +906,6 @@ void Job::return_engine() {
 // ---------------------------------------------------------------------------
 Job::~Job() {
     if (own_engine_) cudaStreamSynchronize(own_engine_->stream());
-    if (apply_graph_) cudaGraphExecDestroy(apply_graph_);
     return_engine();
     stream_ = nullptr;
     RoundBuffers &r = rb_;
@@ -938,18 +936,27 @@ Job::~Job() {
     dfree(jc_.partition);
     dfree(jc_.peel_idx);
     dfree(jc_.upd_list);
-    dfree(d_state_);
     dfree(d_red_);
+    dfree(d_ticket_);
     dfree(d_unc_);
     dfree(d_nunc_);
     dfree(d_lut_);
     dfree(d_hist_);
+    hfree(h_lut_);
+    hfree(h_hist_);
+    hfree(h_nunc_);
+    dfree(jr_.mcrade);
+    dfree(jr_.approx);
+    dfree(jr_.wimpy);
+    dfree(jr_.last_upd);
+    dfree(jr_.sc);
+    dfree(jr_.sp_lengths);
+    if (ev_chk_) cudaEventDestroy(ev_chk_);
     dfree(tk_.hist);
     dfree(tk_.state);
     dfree(tk_.cand);
     hfree(tk_.h_state);
     hfree(tk_.h_cand);
-    hfree(h_state_);
     hfree(h_red_);
     hfree(h_sc_);
     hfree(h_sp_);
@@ -971,6 +978,7 @@ int Job::alloc_round(uint32_t max_samples, uint64_t rec_cap) {
     RK(dmalloc(&r.pred, max_samples));
     RK(dmalloc(&r.node_cnt, n_));
     RK(dmalloc(&r.n_touched, 8));
+    CK(cudaMemset(r.n_touched, 0, 8 * sizeof(uint32_t)));
     RK(dmalloc(&r.inv_np, max_samples));
     r.n_large = r.n_touched + 1;
     r.rec_cursor = nullptr;
@@ -1002,6 +1010,7 @@ int Job::grow_records(uint64_t cap) {
 uint64_t Job::device_bytes() const {
     const uint64_t n = n_;
     uint64_t b = n * (8 + 8 + 8 * kTrials + 4 + 1 + 4 + 4 + 4 + 4);
+    if (p_.k == 0) b += n * (8 * kTrials + 8 + 8 + 4);  // the round journal
     b += (uint64_t)kRoundSamples * 36 + rb_.rec_cap * (12 + 8) +
          std::min<uint64_t>(rb_.rec_cap, n) * 8;
     return b;
@@ -1039,14 +1048,28 @@ int Job::init() {
     RK(dmalloc(&jc_.partition, n));
     RK(dmalloc(&jc_.peel_idx, n));
     RK(dmalloc(&jc_.upd_list, n));
-    RK(dmalloc(&d_state_, 1));
+    if (p_.k == 0) {
+        RK(dmalloc(&jr_.mcrade, (uint64_t)n * kTrials));
+        RK(dmalloc(&jr_.approx, n));
+        RK(dmalloc(&jr_.wimpy, n));
+        RK(dmalloc(&jr_.last_upd, n));
+        RK(dmalloc(&jr_.sc, 1));
+        RK(dmalloc(&jr_.sp_lengths, (uint64_t)g_->diameter + 1));
+        CK(cudaEventCreateWithFlags(&ev_chk_, cudaEventDisableTiming));
+    }
     RK(dmalloc(&d_red_, 1));
+    RK(dmalloc(&d_ticket_, 1));
     RK(dmalloc(&d_unc_, kUncertainCap));
     RK(dmalloc(&d_nunc_, 1));
-    RK(hmalloc(&h_state_, kArgRing));
     RK(hmalloc(&h_red_, 1));
     RK(hmalloc(&h_sc_, 1));
     RK(hmalloc(&h_sp_, (size_t)g_->diameter + 1));
+    RK(hmalloc(&h_nunc_, 1));
+    // the check kernel writes its results straight into these pinned buffers
+    CK(cudaHostGetDevicePointer(reinterpret_cast<void **>(&readback_.red), h_red_, 0));
+    CK(cudaHostGetDevicePointer(reinterpret_cast<void **>(&readback_.sc), h_sc_, 0));
+    CK(cudaHostGetDevicePointer(reinterpret_cast<void **>(&readback_.sp), h_sp_, 0));
+    CK(stop_reduce_init(d_red_, d_ticket_, cudaStreamLegacy));
     CK(cudaMemset(jc_.approx, 0, sizeof(double) * n));
     CK(cudaMemset(jc_.wimpy, 0, sizeof(double) * n));
     CK(cudaMemset(jc_.mcrade, 0, sizeof(long long) * (uint64_t)n * kTrials));
@@ -1062,31 +1085,21 @@ int Job::init() {
     return SILVAN_OK;
 }
 
-int Job::capture_apply(cudaStream_t stream) {
-    if (apply_graph_) return SILVAN_OK;
-    cudaGraph_t g = nullptr;
-    std::lock_guard<std::mutex> cl(capture_mutex());
-    CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
-    cudaError_t e1 = apply_round(d_state_, rb_.n_touched, stream);
-    cudaError_t e2 = cudaStreamEndCapture(stream, &g);
-    CK(e1);
-    CK(e2);
-    cudaError_t e3 = cudaGraphInstantiate(&apply_graph_, g, 0);
-    cudaGraphDestroy(g);
-    CK(e3);
-    return SILVAN_OK;
-}
-
 // Commits samples [lo, hi) (indices into the drawn range r) whose raw outputs
 // the engine left in rb_, in apply sub-rounds of at most kLargeBucket samples.
-int Job::apply_range(const JobRequest &r, uint32_t lo, uint32_t hi, uint64_t n_records) {
-    RK(capture_apply(stream_));
+int Job::apply_range(const JobRequest &r, uint32_t lo, uint32_t hi, uint64_t n_records,
+                     bool journal) {
+    if (journal && (hi - lo > kLargeBucket || !jr_.approx)) {
+        set_error("a journaled commit round must be a single sub-round");
+        return SILVAN_E_STATE;
+    }
     for (uint32_t a0 = lo; a0 < hi; a0 += kLargeBucket) {
-        ApplyState &st = h_state_[arg_slot_];
-        arg_slot_ = (arg_slot_ + 1) % kArgRing;
+        ApplyState st{};
         st.rb = rb_;
         st.jc = jc_;
+        st.jr = jr_;
         ApplyArgs &a = st.a;
+        a.journal = journal ? 1 : 0;
         a.n = n_;
         a.n_records = (uint32_t)n_records;
         a.seed = p_.seed;
@@ -1096,11 +1109,8 @@ int Job::apply_range(const JobRequest &r, uint32_t lo, uint32_t hi, uint64_t n_r
         a.pass = r.pass;
         a.track_cross = r.track_cross ? 1 : 0;
         a.D = g_->diameter;
-        CK(cudaMemcpyAsync(d_state_, &st, sizeof(ApplyState), cudaMemcpyHostToDevice, stream_));
-        CK(cudaGraphLaunch(apply_graph_, stream_));
+        CK(apply_round(st, stream_));
         launches += kApplyRoundKernels;
-        // the pinned argument ring is reused after kArgRing sub-rounds
-        if (arg_slot_ == 0) CK(cudaStreamSynchronize(stream_));
     }
     return SILVAN_OK;
 }
@@ -1112,6 +1122,10 @@ int Job::sync_scalars(JobScalars &sc) {
     CK(cudaMemcpyAsync(h_sc_, jc_.sc, sizeof(JobScalars), cudaMemcpyDeviceToHost, stream_));
     CK(cudaStreamSynchronize(stream_));
     sc = *h_sc_;
+    return scalars_error(sc);
+}
+
+int Job::scalars_error(const JobScalars &sc) {
     if (sc.error != 0) {
         const char *what = sc.error == SILVAN_E_OVERFLOW
                                ? "a sample's 64-bit path count wrapped to 0 (the reference "
@@ -1146,11 +1160,55 @@ void Job::flush() {
 }
 
 // Empirical peeling (silvan/src/Probabilistic.cpp:853-871).
-int Job::peel(double a, bool enabled) {
+// The end of pass 1 in one round trip: one kernel computes every node's
+// peeling index and their histogram (Probabilistic.cpp:853-889) and writes
+// the histogram, the scalars (sc1_) and the path-length counts (sp) to
+// host-mapped memory.  Nodes whose index the device's log could have moved
+// are recomputed with the C library's log, and the histogram again, before
+// the partitions are numbered.
+int Job::peel(double a, bool enabled, std::vector<uint64_t> &sp) {
     const uint32_t n = n_;
+    const uint32_t D = g_->diameter;
     const double ms = (double)pass_samples_;
     part_ids_.clear();
     part_count_.clear();
+    auto host_idx = [&](double w) {
+        double emp_w = w / ms;
+        double min_inv = fmin(1. / emp_w, ms);
+        return (int)(log(min_inv) / log(a) + 1);
+    };
+    int32_t idx_min = 0, nbins = 0;
+    if (enabled) {
+        // the indices lie in [1, log(m)/log(a) + 1]
+        idx_min = std::min(0, host_idx(ms));
+        const int32_t idx_max = std::max(host_idx(0.0), host_idx(ms)) + 2;
+        nbins = idx_max - idx_min + 1;
+        if (nbins > (1 << 22)) {
+            set_error("empirical peeling parameter too close to 1");
+            return SILVAN_E_BADARG;
+        }
+        if ((uint32_t)nbins > hist_cap_) {
+            dfree(d_hist_);
+            hfree(h_hist_);
+            dfree(d_lut_);
+            hfree(h_lut_);
+            RK(dmalloc(&d_hist_, nbins));
+            RK(hmalloc(&h_hist_, nbins));
+            RK(dmalloc(&d_lut_, nbins));
+            RK(hmalloc(&h_lut_, nbins));
+            hist_cap_ = (uint32_t)nbins;
+        }
+    }
+    Pass1Readback out{readback_.sc, readback_.sp, nullptr, nullptr};
+    CK(cudaHostGetDevicePointer(reinterpret_cast<void **>(&out.n_unc), h_nunc_, 0));
+    if (enabled) CK(cudaHostGetDevicePointer(reinterpret_cast<void **>(&out.hist), h_hist_, 0));
+    CK(pass1_readback(jc_, n, ms, a, idx_min, nbins, d_hist_, d_unc_, d_nunc_, kUncertainCap, D,
+                      d_ticket_, out, stream_));
+    launches += 1;
+    CK(cudaStreamSynchronize(stream_));
+    sc1_ = *h_sc_;
+    RK(scalars_error(sc1_));
+    sp.assign(h_sp_, h_sp_ + D + 1);
     if (!enabled) {
         CK(cudaMemsetAsync(jc_.partition, 0, sizeof(int32_t) * n, stream_));
         part_ids_.push_back(0);
@@ -1159,53 +1217,36 @@ int Job::peel(double a, bool enabled) {
         part_host_.assign(n, 0);
         return SILVAN_OK;
     }
-    CK(peel_index(jc_, n, ms, a, d_unc_, d_nunc_, kUncertainCap, stream_));
-    launches += 1;
-    uint32_t nunc = 0;
-    CK(cudaMemcpyAsync(&nunc, d_nunc_, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream_));
-    CK(cudaStreamSynchronize(stream_));
-    auto host_idx = [&](double w) {
-        double emp_w = w / ms;
-        double min_inv = fmin(1. / emp_w, ms);
-        return (int)(log(min_inv) / log(a) + 1);
-    };
-    if (nunc > kUncertainCap) {
-        std::vector<double> w(n);
-        std::vector<int32_t> idx(n);
-        CK(cudaMemcpy(w.data(), jc_.wimpy, sizeof(double) * n, cudaMemcpyDeviceToHost));
-        for (uint32_t i = 0; i < n; i++) idx[i] = host_idx(w[i]);
-        CK(cudaMemcpy(jc_.peel_idx, idx.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice));
-    } else if (nunc > 0) {
-        std::vector<uint32_t> unc(nunc);
-        CK(cudaMemcpy(unc.data(), d_unc_, sizeof(uint32_t) * nunc, cudaMemcpyDeviceToHost));
-        for (uint32_t v : unc) {
-            double w;
-            CK(cudaMemcpy(&w, jc_.wimpy + v, sizeof(double), cudaMemcpyDeviceToHost));
-            int32_t idx = host_idx(w);
-            CK(cudaMemcpy(jc_.peel_idx + v, &idx, sizeof(int32_t), cudaMemcpyHostToDevice));
+    const uint32_t nunc = *h_nunc_;
+    std::vector<uint32_t> hist(h_hist_, h_hist_ + nbins);
+    if (nunc > 0) {
+        if (nunc > kUncertainCap) {
+            std::vector<double> w(n);
+            std::vector<int32_t> idx(n);
+            CK(cudaMemcpy(w.data(), jc_.wimpy, sizeof(double) * n, cudaMemcpyDeviceToHost));
+            for (uint32_t i = 0; i < n; i++) idx[i] = host_idx(w[i]);
+            CK(cudaMemcpy(jc_.peel_idx, idx.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice));
+        } else {
+            std::vector<uint32_t> unc(nunc);
+            CK(cudaMemcpy(unc.data(), d_unc_, sizeof(uint32_t) * nunc, cudaMemcpyDeviceToHost));
+            for (uint32_t v : unc) {
+                double w;
+                CK(cudaMemcpy(&w, jc_.wimpy + v, sizeof(double), cudaMemcpyDeviceToHost));
+                int32_t idx = host_idx(w);
+                CK(cudaMemcpy(jc_.peel_idx + v, &idx, sizeof(int32_t), cudaMemcpyHostToDevice));
+            }
         }
+        CK(peel_hist(jc_, n, idx_min, nbins, d_hist_, stream_));
+        launches += 1;
+        CK(cudaMemcpyAsync(hist.data(), d_hist_, sizeof(uint32_t) * nbins, cudaMemcpyDeviceToHost,
+                           stream_));
+        CK(cudaStreamSynchronize(stream_));
     }
-    // the indices lie in [1, log(m)/log(a) + 1]
-    const int32_t idx_min = std::min(0, host_idx(ms));
-    const int32_t idx_max = std::max(host_idx(0.0), host_idx(ms)) + 2;
-    const int32_t nbins = idx_max - idx_min + 1;
-    if (nbins > (1 << 22)) {
-        set_error("empirical peeling parameter too close to 1");
-        return SILVAN_E_BADARG;
-    }
-    dfree(d_hist_);
-    RK(dmalloc(&d_hist_, nbins));
-    CK(peel_hist(jc_, n, idx_min, nbins, d_hist_, stream_));
-    launches += 1;
-    std::vector<uint32_t> hist(nbins);
-    CK(cudaMemcpyAsync(hist.data(), d_hist_, sizeof(uint32_t) * nbins, cudaMemcpyDeviceToHost,
-                       stream_));
-    CK(cudaStreamSynchronize(stream_));
-    std::vector<int32_t> lut(nbins, 0);
     int dense = 0;
     for (int32_t b = 0; b < nbins; b++) {
+        h_lut_[b] = 0;
         if (hist[b]) {
-            lut[b] = dense++;
+            h_lut_[b] = dense++;
             part_ids_.push_back(b + idx_min);
             part_count_.push_back(hist[b]);
         }
@@ -1215,9 +1256,7 @@ int Job::peel(double a, bool enabled) {
         set_error("more than 128 non-empty peeling partitions");
         return SILVAN_E_BADARG;
     }
-    dfree(d_lut_);
-    RK(dmalloc(&d_lut_, nbins));
-    CK(cudaMemcpy(d_lut_, lut.data(), sizeof(int32_t) * nbins, cudaMemcpyHostToDevice));
+    CK(cudaMemcpyAsync(d_lut_, h_lut_, sizeof(int32_t) * nbins, cudaMemcpyHostToDevice, stream_));
     CK(peel_map(jc_, n, d_lut_, idx_min, nbins, nullptr, stream_));
     launches += 1;
     if (!absolute_) {  // the top-k test looks partitions up per ranked node
@@ -1382,7 +1421,29 @@ bool Job::check_topk(std::string &outs) {
 }
 
 // compute_finished_mcrade (silvan/src/Probabilistic.cpp:251-414).
+// The device part of a check: one kernel writes the reduction, the
+// shortest-path lengths and the scalars to host-mapped memory; ev_chk_ marks
+// its end.
+int Job::stop_check_enqueue() {
+    StopReadback out = readback_;
+    if (!absolute_) out.sp = nullptr;
+    CK(stop_reduce(jc_, nparts_, g_->diameter, d_red_, d_ticket_, out, stream_));
+    launches += 1;
+    if (ev_chk_) CK(cudaEventRecord(ev_chk_, stream_));
+    return SILVAN_OK;
+}
+
 int Job::stop_check(bool &stop) {
+    RK(stop_check_enqueue());
+    return stop_check_finish(stop);
+}
+
+// The host part: waits for the reads of stop_check_enqueue only (work queued
+// after them keeps running).
+int Job::stop_check_finish(bool &stop) {
+    if (ev_chk_) CK(cudaEventSynchronize(ev_chk_));
+    else CK(cudaStreamSynchronize(stream_));
+    RK(scalars_error(*h_sc_));
     std::ostringstream out;
     checks_++;
     const double ms = (double)pass_samples_;
@@ -1392,16 +1453,6 @@ int Job::stop_check(bool &stop) {
     out << "\n";
     out << "EVALUATING STOPPING CONDITION at iteration " << iteration_ << " (m=" << pass_samples_
         << ", d=" << dpb << ")" << "\n";
-    const long long init = -(long long)pass_samples_;
-    CK(stop_reduce(jc_, nparts_, init, d_red_, stream_));
-    launches += 2;
-    // the reduction, the shortest-path lengths and the scalars in one round trip
-    CK(cudaMemcpyAsync(h_red_, d_red_, sizeof(StopReduction), cudaMemcpyDeviceToHost, stream_));
-    if (absolute_)
-        CK(cudaMemcpyAsync(h_sp_, jc_.sp_lengths, sizeof(uint64_t) * ((size_t)g_->diameter + 1),
-                           cudaMemcpyDeviceToHost, stream_));
-    JobScalars sc;
-    RK(sync_scalars(sc));
     const StopReduction &R = *h_red_;
     if (absolute_) {
         const std::vector<uint64_t> sp(h_sp_, h_sp_ + g_->diameter + 1);
@@ -1428,8 +1479,9 @@ int Job::stop_check(bool &stop) {
         const bool zeros = R.touched[i] < part_count_[i];
         double avg = 0.0;
         for (int j = 0; j < kTrials; j++) {
-            const long long mj = zeros ? std::max(R.mc_max[i * kTrials + j], 0ll)
-                                       : R.mc_max[i * kTrials + j];
+            // the reduction starts each maximum at -n_pairs
+        const long long mr = std::max(R.mc_max[i * kTrials + j], -(long long)pass_samples_);
+        const long long mj = zeros ? std::max(mr, 0ll) : mr;
             avg += mj / (double)kTrials;
         }
         avg = avg / ms;
@@ -1470,12 +1522,12 @@ int Job::stop_check(bool &stop) {
     return SILVAN_OK;
 }
 
+// Pass 2 starts from zero counters.  Pass 1 changes approx, wimpy and
+// last_upd of the nodes on upd_list only, and no mcrade, so only those are
+// written (before the scalars, which hold the list's length, are zeroed).
 void Job::reset_pass2_counters() {
-    const uint32_t n = n_;
-    cudaMemsetAsync(jc_.approx, 0, sizeof(double) * n, stream_);
-    cudaMemsetAsync(jc_.wimpy, 0, sizeof(double) * n, stream_);
-    cudaMemsetAsync(jc_.mcrade, 0, sizeof(long long) * (uint64_t)n * kTrials, stream_);
-    cudaMemsetAsync(jc_.last_upd, 0, sizeof(uint32_t) * n, stream_);
+    reset_updated(jc_, stream_);
+    launches += 1;
 }
 
 // ---------------------------------------------------------------------------
@@ -1592,14 +1644,14 @@ int Job::finish_pass1() {
     const double eps = p_.eps, delta = p_.delta;
     const uint64_t P1 = pass_samples_;
     p1_samples_ = P1;
-    RK(sync_scalars(sc1_));
+    // empirical peeling (:853-889), with the scalars and path-length counts
+    std::vector<uint64_t> sp;
+    RK(peel(peel_a_, peel_on_, sp));
     double sup_bcest, sup_wv;
     std::memcpy(&sup_bcest, &sc1_.sup_approx_bits, sizeof(double));
     std::memcpy(&sup_wv, &sc1_.sup_wimpy_bits, sizeof(double));
     std::ostringstream out;
     out << "First pass finished after " << P1 << " iteration" << "\n";
-    // empirical peeling (:853-889)
-    RK(peel(peel_a_, peel_on_));
     out << "number_of_non_empty_partitions  " << nparts_ << "\n";
     for (int i = 0; i < nparts_; i++)
         out << "  part. w. index  " << part_ids_[i] << " has " << part_count_[i]
@@ -1610,8 +1662,6 @@ int Job::finish_pass1() {
     // bounds and the alpha switch (:906-942)
     double mns = 0.;
     if (absolute_) {
-        std::vector<uint64_t> sp;
-        RK(read_sp_lengths(sp));
         AvgDiamBound adb = upper_bound_avg_diameter(sp, D, delta / 8., P1);
         out << "avg_diam_: " << adb.avg << "\n";
         out << "avg_diam_upperbound_b: " << adb.ub_b << "\n";
@@ -1718,14 +1768,23 @@ int Job::on_drawn(const JobRequest &r, uint64_t n_records) {
         }
         if (pass_samples_ < target_) break;  // the next point lies beyond the drawn range
         const Phase ph = phase_;
-        RK(evaluate());
+        ov_.on = true;
+        ov_.rc = rc;
+        ov_.g0 = g0;
+        ov_.g1 = g1;
+        ov_.n_records = n_records;
+        const int ev = evaluate();
+        ov_.on = false;
+        RK(ev);
         if (done()) break;
         if (phase_ != ph) {
             // pass 1 ended: the rest of the draw is pass 2's if drawn with its alpha
             if (alpha_ != r.alpha) break;
             continue;
         }
-        if (base_global_ + pass_samples_ != c_hi) break;  // pass 1 redrawn from the start
+        // pass 1 redrawn from the start (the next round of a check that let
+        // the run go on may already be committed: pass_samples_ moved on)
+        if (base_global_ + pass_samples_ < c_hi) break;
     }
     CK(cudaEventRecord(ev_commit_[1], stream_));
     CK(cudaEventSynchronize(ev_commit_[1]));
@@ -1735,6 +1794,36 @@ int Job::on_drawn(const JobRequest &r, uint64_t n_records) {
         commit_ms_ += ms;
         if (done()) result_.time_apply_s = commit_ms_ / 1000.0;  // the run ended in this call
     }
+    return SILVAN_OK;
+}
+
+// Pass 2 of absolute mode, between the device part of a check and its host
+// part: commits the round up to the schedule point that follows the check
+// when the check lets the run go on and leaves omega and the last stopping
+// size where they are, with a journal (ov_ records the round).  The host
+// evaluates the check meanwhile; evaluate() keeps the round if the point
+// comes out the same and undoes it otherwise.  The samples must be in the
+// drawn range and fit one commit sub-round.
+int Job::speculate() {
+    ov_.spec_lo = ov_.spec_hi = 0;
+    if (!ov_.on || !absolute_ || !jr_.approx || phase_ != kPass2 || ov_.rc.pass != 2 ||
+        ov_.rc.alpha != alpha_)
+        return SILVAN_OK;
+    const uint64_t ns = (uint64_t)(next_stop_ * 1.2);
+    const uint64_t t = pass2_target(pass_samples_, p_.m_hat != 0, omega_, ns, last_stop_);
+    if (t <= pass_samples_ || t - pass_samples_ > kLargeBucket) return SILVAN_OK;
+    const uint64_t cur = base_global_ + pass_samples_, hi = base_global_ + t;
+    if (cur < ov_.g0 || hi > ov_.g1) return SILVAN_OK;
+    RK(apply_range(ov_.rc, (uint32_t)(cur - ov_.g0), (uint32_t)(hi - ov_.g0), ov_.n_records, true));
+    ov_.spec_lo = pass_samples_;
+    ov_.spec_hi = t;
+    return SILVAN_OK;
+}
+
+int Job::undo_speculation() {
+    CK(undo_round(rb_, jc_, jr_, 2, g_->diameter, stream_));
+    launches += 1;
+    ov_.spec_lo = ov_.spec_hi = 0;
     return SILVAN_OK;
 }
 
@@ -1792,7 +1881,9 @@ int Job::evaluate() {
         stop = true;
         stop_reason_ = 2;
     } else if ((double)pass_samples_ < last_stop_ && pass_samples_ >= next_stop_) {
-        RK(stop_check(stop));
+        RK(stop_check_enqueue());
+        RK(speculate());
+        RK(stop_check_finish(stop));
         if (stop) {
             std::ostringstream o;
             o << "MCRADE STOPS after seconds " << now_seconds() - t_start_ << "\n";
@@ -1807,8 +1898,18 @@ int Job::evaluate() {
     }
     if (!stop) {
         target_ = pass2_target(pass_samples_, p_.m_hat != 0, omega_, next_stop_, last_stop_);
+        if (ov_.spec_hi) {
+            // the journaled round ends at the point the check left: it stands
+            if (target_ == ov_.spec_hi && pass_samples_ == ov_.spec_lo) {
+                pass_samples_ = ov_.spec_hi;
+                ov_.spec_lo = ov_.spec_hi = 0;
+            } else {
+                RK(undo_speculation());
+            }
+        }
         return SILVAN_OK;
     }
+    if (ov_.spec_hi) RK(undo_speculation());
     // ---- end of the run (:1103-1138) ---------------------------------------
     CK(cudaEventRecord(ev_run_[1], stream_));
     JobScalars sc2;

@@ -266,14 +266,19 @@ class Job {
   private:
     enum Phase { kInit, kPass1, kPass2, kDone };
     int alloc_round(uint32_t max_samples, uint64_t rec_cap);
-    int capture_apply(cudaStream_t stream);
-    int apply_range(const JobRequest &r, uint32_t lo, uint32_t hi, uint64_t n_records);
+    int apply_range(const JobRequest &r, uint32_t lo, uint32_t hi, uint64_t n_records,
+                    bool journal = false);
     int evaluate();
+    int speculate();
+    int undo_speculation();
     int sync_scalars(JobScalars &sc);
     int read_sp_lengths(std::vector<uint64_t> &out);
-    int peel(double a, bool enabled);
+    int peel(double a, bool enabled, std::vector<uint64_t> &sp);
     int finish_pass1();
     int stop_check(bool &stop);
+    int stop_check_enqueue();
+    int stop_check_finish(bool &stop);
+    int scalars_error(const JobScalars &sc);
     int ranking(std::vector<uint32_t> &el, std::vector<double> &val);
     bool check_topk(std::string &out);
     void reset_pass2_counters();
@@ -288,18 +293,31 @@ class Job {
     RoundBuffers rb_{};
     uint32_t n_ = 0;
     JobCounters jc_{};
-    ApplyState *d_state_ = nullptr;
-    ApplyState *h_state_ = nullptr;  // pinned ring of kArgRing entries
-    uint32_t arg_slot_ = 0;
-    cudaGraphExec_t apply_graph_ = nullptr;
-    StopReduction *d_red_ = nullptr;
+    StopReduction *d_red_ = nullptr;  // the check kernel's accumulator (neutral between checks)
+    uint32_t *d_ticket_ = nullptr;
+    StopReadback readback_{};         // device view of h_red_, h_sc_, h_sp_
     StopReduction *h_red_ = nullptr;  // pinned
     JobScalars *h_sc_ = nullptr;      // pinned
     uint64_t *h_sp_ = nullptr;        // pinned, diameter + 1 shortest-path lengths
     uint32_t *d_unc_ = nullptr, *d_nunc_ = nullptr;
     int32_t *d_lut_ = nullptr;
     uint32_t *d_hist_ = nullptr;
+    int32_t *h_lut_ = nullptr;    // pinned
+    uint32_t *h_hist_ = nullptr;  // pinned, written by the end-of-pass-1 kernel
+    uint32_t *h_nunc_ = nullptr;  // pinned, likewise
+    uint32_t hist_cap_ = 0;
     TopkBuffers tk_{};  // top-k mode: device selection of the ranking
+    // absolute mode, pass 2: the round after a check is committed (journaled)
+    // while the host evaluates the check, and undone if the check stops the
+    // run or moves the next schedule point
+    RoundJournal jr_{};
+    cudaEvent_t ev_chk_ = nullptr;  // the check's reads have landed
+    struct Overlap {
+        bool on = false;      // on_drawn is committing a drawn range
+        JobRequest rc{};      // that range, as pass 2 commits it
+        uint64_t g0 = 0, g1 = 0, n_records = 0;
+        uint64_t spec_lo = 0, spec_hi = 0;  // pass samples of the journaled round (0, 0: none)
+    } ov_;
     cudaEvent_t ev_run_[2] = {nullptr, nullptr};
     FILE *sink_ = nullptr;
     std::string out_;  // pending status lines
