@@ -90,7 +90,12 @@ typedef struct {
                             are unaffected): 0 = default (2^20, far above
                             any real wait), 0xffffffff = no polls at all (a
                             hook for tests of that failure path)            */
-    uint32_t pad0;
+    uint32_t serial_checks; /* absolute mode: 0 = default, the commit of the
+                            samples after a stopping-rule check runs while
+                            the host evaluates the check (and is undone if
+                            the check stops the run); 1 = each check is
+                            evaluated before any later sample is committed.
+                            The results are the same.                       */
 } silvan_params_t;
 
 /* Predecessor choice of the random backtrack.  REFERENCE is the rule of
@@ -142,7 +147,8 @@ typedef struct {
     uint64_t samples_drawn;      /* samples drawn, speculative ones included */
     uint32_t assisted_levels;    /* BFS levels expanded by several CTAs (own
                                     engine; see silvan_params_t::assist_items) */
-    uint32_t pad0;
+    uint32_t overlapped_checks;  /* checks during whose evaluation the next
+                                    samples were committed (and kept)      */
     uint64_t helper_tiles;       /* tiles of those levels done by helpers    */
 } silvan_result_t;
 

@@ -61,7 +61,7 @@ class Params(C.Structure):
                 ("verbose", C.c_double), ("np_cap", C.c_uint32), ("slots", C.c_uint32),
                 ("threads", C.c_uint32), ("block", C.c_uint32),
                 ("backtrack", C.c_uint32), ("assist_items", C.c_uint32),
-                ("wait_polls", C.c_uint32), ("pad0", C.c_uint32)]
+                ("wait_polls", C.c_uint32), ("serial_checks", C.c_uint32)]
 
 
 class Result(C.Structure):
@@ -82,7 +82,7 @@ class Result(C.Structure):
                 ("pred_entries", C.c_uint64), ("kernel_launches", C.c_uint64),
                 ("sampler_launches", C.c_uint32), ("sampler_block", C.c_uint32),
                 ("samples_drawn", C.c_uint64), ("assisted_levels", C.c_uint32),
-                ("pad0", C.c_uint32), ("helper_tiles", C.c_uint64)]
+                ("overlapped_checks", C.c_uint32), ("helper_tiles", C.c_uint64)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}
@@ -382,12 +382,15 @@ class Probabilistic:
     remain, 8 x once all are taken, 0xFFFFFFFF =
     never) and `wait_polls` (polls after which a wait between CTAs that
     share a level gives up and the job fails with E_TIMEOUT; 0 = default,
-    0xFFFFFFFF = no polls, a hook for tests of that path).  Only `seed`,
+    0xFFFFFFFF = no polls, a hook for tests of that path) and
+    `serial_checks` (evaluate each stopping-rule check before committing
+    later samples, instead of overlapping the two).  Only `seed`,
     `backtrack` and, in top-k mode, `threads` change the results."""
 
     def __init__(self, graph: Graph, eps, delta, k=0, alpha=2.3, alpha_given=False, a=2.0,
                  m_hat=True, seed=42, form="batched", verbose=0.0, np_cap=0, slots=0,
-                 threads=1, block=0, backtrack="reference", assist_items=0, wait_polls=0):
+                 threads=1, block=0, backtrack="reference", assist_items=0, wait_polls=0,
+                 serial_checks=False):
         lib = load()
         p = Params()
         lib.silvan_params_default(C.byref(p))
@@ -398,6 +401,7 @@ class Probabilistic:
         p.np_cap, p.slots, p.threads, p.block = np_cap, slots, threads, block
         p.assist_items = assist_items
         p.wait_polls = wait_polls
+        p.serial_checks = int(serial_checks)
         p.backtrack = {"reference": BACKTRACK_REFERENCE,
                        "sigma": BACKTRACK_SIGMA_WEIGHTED}[backtrack]
         self.graph = graph

@@ -93,6 +93,7 @@ void silvan_params_default(silvan_params_t *p) {
     p->backtrack = SILVAN_BACKTRACK_REFERENCE;
     p->assist_items = 0;
     p->wait_polls = 0;
+    p->serial_checks = 0;
 }
 
 const char *silvan_last_error(void) { return last_error_cstr(); }

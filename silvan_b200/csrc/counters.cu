@@ -86,14 +86,22 @@ __device__ bool grid_barrier(uint32_t *bar) {
 
 __device__ void bucket_count(const RoundBuffers &rb, const ApplyArgs &a) {
     const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
-    // per sample: the Rademacher signs (pass 2) and 1 / num_paths, the factor
-    // every record of the sample is multiplied by (Probabilistic.cpp:502)
-    for (uint32_t s = a.lo + tid; s < a.hi; s += nth) {
-        if (a.pass == 2) rb.signs[s] = rademacher_mask(a.seed, a.first_sample + s);
-        rb.inv_np[s] = __ddiv_rn(1.0, (double)rb.np[s]);
+    const uint32_t lane = threadIdx.x & 31;
+    // per sample, one warp: the Rademacher signs (pass 2; lane j draws trial
+    // j, as rademacher_mask does) and 1 / num_paths, the factor every record
+    // of the sample is multiplied by (Probabilistic.cpp:502)
+    for (uint32_t s = a.lo + (tid >> 5); s < a.hi; s += nth >> 5) {
+        if (a.pass == 2) {
+            bool plus = false;
+            if (lane < (uint32_t)kTrials)
+                plus = philox_lo32(a.seed, a.first_sample + s, kStreamRademacher, lane) %
+                           100000000u >= 50000000u;
+            const uint32_t m = __ballot_sync(0xffffffffu, plus);
+            if (lane == 0) rb.signs[s] = m;
+        }
+        if (lane == 31) rb.inv_np[s] = __ddiv_rn(1.0, (double)rb.np[s]);
     }
     const uint32_t R = round_records(rb, a);
-    const uint32_t lane = threadIdx.x & 31;
     // warp-uniform loop: the first record of a node is appended to the
     // touched list with one counter increment per warp (a single counter
     // that every warp hits would serialise the whole phase)
@@ -325,6 +333,7 @@ struct CommitSmem {
     FoldScratch fsc[kCommitThreads / 32];
 };
 constexpr size_t kCommitSmem = sizeof(CommitSmem);
+constexpr int kLoads = 8;  // bucket entries a lane of warp 0 loads at once
 constexpr uint32_t kSmallWarps = kCommitThreads / 32 - 1;  // warps 1.. of each CTA
 
 // Buckets of at most 32 entries, on warps 1.. of every CTA: touched node t
@@ -390,10 +399,22 @@ __device__ void apply_large(const RoundBuffers &rb, const JobCounters &jc, const
         const NodeState st = fold_load(jc, jr, a, node, t);
         for (uint32_t w = w0; w < w1; w++) sm.bits[w] = 0u;
         __syncwarp();
-        for (uint32_t i = lane; i < b; i += 32) {
-            const uint32_t sidx = (uint32_t)(__ldcg(&rb.entries[b0 + i]) >> 32) - a.lo;
-            if (sidx < S) atomicOr(&sm.bits[sidx >> 5], 1u << (sidx & 31));
-            else atomicCAS(&jc.sc->error, 0, SILVAN_E_STATE);
+        // the bucket's entries kLoads at a time per lane, all loads in
+        // flight before their uses
+        for (uint32_t i0 = 0; i0 < b; i0 += 32 * kLoads) {
+            unsigned long long e[kLoads];
+#pragma unroll
+            for (int j = 0; j < kLoads; j++) {
+                const uint32_t i = i0 + (uint32_t)j * 32 + lane;
+                e[j] = i < b ? __ldcg(&rb.entries[b0 + i]) : 0ull;
+            }
+#pragma unroll
+            for (int j = 0; j < kLoads; j++) {
+                if (i0 + (uint32_t)j * 32 + lane >= b) continue;
+                const uint32_t sidx = (uint32_t)(e[j] >> 32) - a.lo;
+                if (sidx < S) atomicOr(&sm.bits[sidx >> 5], 1u << (sidx & 31));
+                else atomicCAS(&jc.sc->error, 0, SILVAN_E_STATE);
+            }
         }
         __syncwarp();
         // exclusive prefix of the words' bit counts (lane L owns words
@@ -411,12 +432,21 @@ __device__ void apply_large(const RoundBuffers &rb, const JobCounters &jc, const
             run += __popc(sm.bits[w]);
         }
         __syncwarp();
-        for (uint32_t i = lane; i < b; i += 32) {
-            const unsigned long long e = __ldcg(&rb.entries[b0 + i]);
-            const uint32_t sidx = (uint32_t)(e >> 32) - a.lo;
-            if (sidx < S) {
-                const uint32_t w = sidx >> 5;
-                sm.sbuf[sm.wpre[w] + __popc(sm.bits[w] & ((1u << (sidx & 31)) - 1u))] = e;
+        for (uint32_t i0 = 0; i0 < b; i0 += 32 * kLoads) {
+            unsigned long long e[kLoads];
+#pragma unroll
+            for (int j = 0; j < kLoads; j++) {
+                const uint32_t i = i0 + (uint32_t)j * 32 + lane;
+                e[j] = i < b ? __ldcg(&rb.entries[b0 + i]) : 0ull;
+            }
+#pragma unroll
+            for (int j = 0; j < kLoads; j++) {
+                if (i0 + (uint32_t)j * 32 + lane >= b) continue;
+                const uint32_t sidx = (uint32_t)(e[j] >> 32) - a.lo;
+                if (sidx < S) {
+                    const uint32_t w = sidx >> 5;
+                    sm.sbuf[sm.wpre[w] + __popc(sm.bits[w] & ((1u << (sidx & 31)) - 1u))] = e[j];
+                }
             }
         }
         __syncwarp();
@@ -652,19 +682,43 @@ __global__ void __launch_bounds__(512) stop_reduce_kernel(JobCounters jc, int np
     const int lane = threadIdx.x & 31;
     const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
     unsigned long long amax = 0, wmax = 0;
-    for (uint32_t t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < T; t += nw) {
-        const uint32_t v = jc.upd_list[t];
-        const int p = jc.partition[v];
-        if (lane < kTrials) {
-            const long long m = jc.mcrade[(uint64_t)v * kTrials + lane];
-            if (m > smc[p * kTrials + lane]) atomicMax(&smc[p * kTrials + lane], m);
-        } else if (lane == kTrials) {
-            const unsigned long long wb = (unsigned long long)__double_as_longlong(jc.wimpy[v]);
-            const unsigned long long ab = (unsigned long long)__double_as_longlong(jc.approx[v]);
-            if (wb > sw[p]) atomicMax(&sw[p], wb);
-            atomicAdd(&st[p], 1u);
-            amax = ab > amax ? ab : amax;
-            wmax = wb > wmax ? wb : wmax;
+    // kNodes nodes per warp at a time, their loads in flight together
+    constexpr int kNodes = 4;
+    for (uint32_t t0 = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t0 < T; t0 += kNodes * nw) {
+        uint32_t v[kNodes];
+        int p[kNodes];
+        long long m[kNodes];
+        unsigned long long wb[kNodes], ab[kNodes];
+#pragma unroll
+        for (int i = 0; i < kNodes; i++) {
+            const uint32_t t = t0 + (uint32_t)i * nw;
+            v[i] = t < T ? jc.upd_list[t] : 0xffffffffu;
+        }
+#pragma unroll
+        for (int i = 0; i < kNodes; i++) {
+            p[i] = 0;
+            m[i] = LLONG_MIN;
+            wb[i] = ab[i] = 0ull;
+            if (v[i] == 0xffffffffu) continue;
+            p[i] = jc.partition[v[i]];
+            if (lane < kTrials) {
+                m[i] = jc.mcrade[(uint64_t)v[i] * kTrials + lane];
+            } else if (lane == kTrials) {
+                wb[i] = (unsigned long long)__double_as_longlong(jc.wimpy[v[i]]);
+                ab[i] = (unsigned long long)__double_as_longlong(jc.approx[v[i]]);
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < kNodes; i++) {
+            if (v[i] == 0xffffffffu) continue;
+            if (lane < kTrials) {
+                if (m[i] > smc[p[i] * kTrials + lane]) atomicMax(&smc[p[i] * kTrials + lane], m[i]);
+            } else if (lane == kTrials) {
+                if (wb[i] > sw[p[i]]) atomicMax(&sw[p[i]], wb[i]);
+                atomicAdd(&st[p[i]], 1u);
+                amax = ab[i] > amax ? ab[i] : amax;
+                wmax = wb[i] > wmax ? wb[i] : wmax;
+            }
         }
     }
     for (int o = 16; o > 0; o >>= 1) {
@@ -678,10 +732,15 @@ __global__ void __launch_bounds__(512) stop_reduce_kernel(JobCounters jc, int np
         if (wmax) atomicMax(reinterpret_cast<unsigned long long *>(&acc->wimpy_all_max), wmax);
     }
     __syncthreads();
+    // every CTA folds the same few hundred words: an atomic only where this
+    // CTA's value is above the accumulator's (most are not), so that the
+    // CTAs do not queue on the same addresses
     for (int i = threadIdx.x; i < nparts * kTrials; i += blockDim.x)
-        if (smc[i] != LLONG_MIN) atomicMax(&acc->mc_max[i], smc[i]);
+        if (smc[i] != LLONG_MIN && smc[i] > __ldcg(&acc->mc_max[i]))
+            atomicMax(&acc->mc_max[i], smc[i]);
     for (int i = threadIdx.x; i < nparts; i += blockDim.x) {
-        if (sw[i]) atomicMax(reinterpret_cast<unsigned long long *>(&acc->wimpy_max[i]), sw[i]);
+        unsigned long long *wm = reinterpret_cast<unsigned long long *>(&acc->wimpy_max[i]);
+        if (sw[i] && sw[i] > __ldcg(wm)) atomicMax(wm, sw[i]);
         if (st[i]) atomicAdd(&acc->touched[i], st[i]);
     }
     __syncthreads();

@@ -788,16 +788,31 @@ int Engine::round(const std::vector<Job *> &jobs, const std::vector<JobRequest> 
     return SILVAN_OK;
 }
 
+// Samples the first launch of the next job of this class draws.  Seeds stop
+// at different schedule points (on R-MAT scale 20 the totals of 60 seeds
+// spread over +-13 % of their mean), so one earlier total is a noisy guess:
+// with fewer than kHintMin totals recorded, 25 % above the last one; with
+// more, 3 % above the largest of the last kHintJobs, which about one job in
+// kHintJobs + 1 exceeds (it then draws its rest in a second launch).
 uint64_t Engine::job_hint(const DeviceGraph *G) const {
     auto it = job_total_.find(G->tune_class());
-    return it == job_total_.end() ? 0 : it->second;
+    if (it == job_total_.end() || it->second.empty()) return 0;
+    const std::deque<uint64_t> &h = it->second;
+    if (h.size() < kHintMin) return h.back() + h.back() / 4;
+    const uint64_t mx = *std::max_element(h.begin(), h.end());
+    return mx + mx / 32;
 }
 
 void Engine::note_job(const DeviceGraph *G, uint64_t used, bool alpha_kept) {
     // only a job whose second pass kept the first pass's alpha can use
     // samples drawn ahead in its first launch
-    if (alpha_kept) job_total_[G->tune_class()] = used;
-    else job_total_.erase(G->tune_class());
+    if (!alpha_kept) {
+        job_total_.erase(G->tune_class());
+        return;
+    }
+    std::deque<uint64_t> &h = job_total_[G->tune_class()];
+    h.push_back(used);
+    while (h.size() > kHintJobs) h.pop_front();
 }
 
 uint32_t Engine::free_samples(const DeviceGraph *G, bool tail_only) const {
@@ -1588,13 +1603,13 @@ bool Job::next_request(JobRequest &r) {
         // would otherwise ask for a launch whose size favours long tails
         uint64_t ahead = phase_ == kPass2 ? lookahead_
                                           : std::min<uint64_t>(lookahead_tail_, 4 * target_);
-        if (phase_ == kPass1 && hint_total_ > target_) {
-            // the last job of this class of graphs used hint_total_ samples
-            // with pass 2 on the same stream: draw that far at once (25 %
-            // more: the stop of another seed lies within a schedule step or
-            // two, and a second launch costs more than the extra samples),
-            // so that one launch usually covers the whole estimation
-            ahead = std::max<uint64_t>(ahead, hint_total_ + hint_total_ / 4 - target_);
+        if (phase_ == kPass1 && hint_total_ > target_ && hint_total_ > pass_samples_) {
+            // the earlier jobs of this class of graphs suggest drawing
+            // hint_total_ samples (Engine::job_hint) with pass 2 on the same
+            // stream: draw that far at once, so that one launch usually
+            // covers the whole estimation (a second launch costs more than
+            // a few extra samples)
+            ahead = std::max<uint64_t>(ahead, hint_total_ - pass_samples_);
         }
         if (phase_ == kPass2 && predicted_stop_ > pass_samples_) {
             // absolute mode after a failed check: up to the schedule point at
@@ -1806,8 +1821,8 @@ int Job::on_drawn(const JobRequest &r, uint64_t n_records) {
 // drawn range and fit one commit sub-round.
 int Job::speculate() {
     ov_.spec_lo = ov_.spec_hi = 0;
-    if (!ov_.on || !absolute_ || !jr_.approx || phase_ != kPass2 || ov_.rc.pass != 2 ||
-        ov_.rc.alpha != alpha_)
+    if (!ov_.on || !absolute_ || !jr_.approx || p_.serial_checks || phase_ != kPass2 ||
+        ov_.rc.pass != 2 || ov_.rc.alpha != alpha_)
         return SILVAN_OK;
     const uint64_t ns = (uint64_t)(next_stop_ * 1.2);
     const uint64_t t = pass2_target(pass_samples_, p_.m_hat != 0, omega_, ns, last_stop_);
@@ -1902,6 +1917,7 @@ int Job::evaluate() {
             // the journaled round ends at the point the check left: it stands
             if (target_ == ov_.spec_hi && pass_samples_ == ov_.spec_lo) {
                 pass_samples_ = ov_.spec_hi;
+                overlapped_checks_++;
                 ov_.spec_lo = ov_.spec_hi = 0;
             } else {
                 RK(undo_speculation());
@@ -1990,6 +2006,7 @@ int Job::evaluate() {
     res.samples_drawn = drawn_;
     res.assisted_levels = own_engine_ ? own_engine_->assisted_levels() : 0;
     res.helper_tiles = own_engine_ ? own_engine_->helper_tiles() : 0;
+    res.overlapped_checks = overlapped_checks_;
     phase_ = kDone;
     return SILVAN_OK;
 }

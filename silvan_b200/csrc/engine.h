@@ -13,6 +13,7 @@
 #include <cstdio>
 #include <mutex>
 #include <string>
+#include <deque>
 #include <unordered_map>
 #include <vector>
 
@@ -207,7 +208,9 @@ class Engine {
         uint32_t samples = 0;  // drawn by the launch
     };
     std::unordered_map<uint64_t, LastLaunch> last_;  // by tune_class()
-    std::unordered_map<uint64_t, uint64_t> job_total_;  // by tune_class(): see job_hint
+    // by tune_class(): the samples of the last kHintJobs jobs (see job_hint)
+    std::unordered_map<uint64_t, std::deque<uint64_t>> job_total_;
+    static constexpr size_t kHintJobs = 8, kHintMin = 4;
 };
 
 class Job {
@@ -354,6 +357,7 @@ class Job {
     uint32_t numresults_topk_ = 0;
     double eps_stop_ = -1;
     uint32_t checks_ = 0;
+    uint32_t overlapped_checks_ = 0;
     double max_num_samples_ = 0;
     uint64_t p1_samples_ = 0;
     JobScalars sc1_{};
