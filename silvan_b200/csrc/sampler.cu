@@ -326,6 +326,9 @@ __device__ void expand_level(const SegDesc &A, SamplerSmem<BLOCK> &s, NodeRec *r
     uint32_t gbase = 0;  // item number of the chunk's first item within the level
     uint32_t sum_local = 0;
     uint32_t hits_local = 0;
+    // ends of the queue and of the meeting list, advanced tile by tile in
+    // every thread alike (thread 0 stores them when the level is done)
+    uint32_t qend = s.end_q, mend = s.nmeet;
     for (uint32_t c0 = lo; c0 < hi; c0 += kChunk) {
         const uint32_t nc = min((uint32_t)kChunk, hi - c0);
         // stage the chunk: row starts, degrees (prefix), sigma
@@ -462,21 +465,24 @@ __device__ void expand_level(const SegDesc &A, SamplerSmem<BLOCK> &s, NodeRec *r
                 }
             }
             __syncthreads();
-            if (warp == 0) {
-                // exclusive offsets over (k, warp) in item order; the tile's
-                // bases; the queue and meeting-list ends advance here (the
-                // next tile reads them only after its own phase-1 barrier)
+            // Every warp turns the counts into exclusive offsets over
+            // (k, warp) in item order (the same sums in every warp) and picks
+            // its own kItems of them by shuffles; no second barrier.  The next
+            // tile writes the counts again only after its own phase-1
+            // barrier, which every warp reaches after reading these.
+            uint32_t oa[kItems], ob[kItems];
+            {
                 constexpr int kE = kItems * kWarps;
                 constexpr int kPerLane = (kE + 31) / 32;
-                uint32_t va[kPerLane], vb[kPerLane];
+                uint32_t pa[kPerLane], pb[kPerLane];
                 uint32_t sa = 0, sb = 0;
 #pragma unroll
                 for (int i = 0; i < kPerLane; i++) {
                     const int e = lane * kPerLane + i;
-                    va[i] = e < kE ? s.warp_a[e] : 0u;
-                    vb[i] = e < kE ? s.warp_b[e] : 0u;
-                    sa += va[i];
-                    sb += vb[i];
+                    pa[i] = e < kE ? s.warp_a[e] : 0u;
+                    pb[i] = e < kE ? s.warp_b[e] : 0u;
+                    sa += pa[i];
+                    sb += pb[i];
                 }
                 uint32_t ia = sa, ib = sb;
 #pragma unroll
@@ -490,31 +496,40 @@ __device__ void expand_level(const SegDesc &A, SamplerSmem<BLOCK> &s, NodeRec *r
                 }
                 const uint32_t an = __shfl_sync(0xffffffffu, ia, 31);
                 const uint32_t am = __shfl_sync(0xffffffffu, ib, 31);
-                const uint32_t qb = s.end_q, mb0 = s.nmeet;
-                __syncwarp();
-                uint32_t ea = qb + ia - sa, eb = mb0 + ib - sb;
+                // this lane's entries: counts -> exclusive offsets
+                uint32_t ea = qend + ia - sa, eb = mend + ib - sb;
 #pragma unroll
                 for (int i = 0; i < kPerLane; i++) {
-                    const int e = lane * kPerLane + i;
-                    if (e < kE) {
-                        s.warp_a[e] = ea;
-                        s.warp_b[e] = eb;
-                    }
-                    ea += va[i];
-                    eb += vb[i];
+                    const uint32_t ca = pa[i], cb = pb[i];
+                    pa[i] = ea;
+                    pb[i] = eb;
+                    ea += ca;
+                    eb += cb;
                 }
-                if (lane == 0) {
-                    s.end_q = qb + an;
-                    s.nmeet = min(mb0 + am, kMeetCap);
-                    if (mb0 + am > kMeetCap && s.status == 0) s.status = SILVAN_E_CAPACITY;
+#pragma unroll
+                for (int k = 0; k < kItems; k++) {
+                    const int e = k * kWarps + warp;
+                    const int owner = e / kPerLane, sub = e % kPerLane;
+                    uint32_t va = pa[0], vb = pb[0];
+#pragma unroll
+                    for (int i = 1; i < kPerLane; i++)
+                        if (sub == i) {
+                            va = pa[i];
+                            vb = pb[i];
+                        }
+                    oa[k] = __shfl_sync(0xffffffffu, va, owner);
+                    ob[k] = __shfl_sync(0xffffffffu, vb, owner);
                 }
+                if (threadIdx.x == 0 && mend + am > kMeetCap && s.status == 0)
+                    s.status = SILVAN_E_CAPACITY;
+                qend += an;
+                mend = min(mend + am, kMeetCap);
             }
-            __syncthreads();
 #pragma unroll
             for (int k = 0; k < kItems; k++) {
                 if (code[k] == 1) {
                     const uint32_t y = ys[k];
-                    queue[s.warp_a[k * kWarps + warp] + rn[k]] = y;
+                    queue[oa[k] + rn[k]] = y;
                     if (single & (1u << k)) {
                         // the only hit: st, cnt = 1, sigma, first = last = key
                         const uint32_t it = t0 + (uint32_t)(k * BLOCK) + threadIdx.x;
@@ -526,7 +541,7 @@ __device__ void expand_level(const SegDesc &A, SamplerSmem<BLOCK> &s, NodeRec *r
                     }
                     sum_local += dg[k];
                 } else if (code[k] == 2) {
-                    const uint32_t pos = s.warp_b[k * kWarps + warp] + rm[k];
+                    const uint32_t pos = ob[k] + rm[k];
                     if (pos < kMeetCap) meet[pos] = make_uint2(xs[k], ys[k]);
                 }
             }
@@ -554,8 +569,10 @@ __device__ void expand_level(const SegDesc &A, SamplerSmem<BLOCK> &s, NodeRec *r
         }
         s.sum_new = sn;
         s.pred_hits += ph;
+        s.end_q = qend;
+        s.nmeet = mend;
     }
-    // the caller's thread 0 consumes sum_new before its next barrier
+    // the caller's thread 0 consumes sum_new and the ends before its next barrier
 }
 
 // ---------------------------------------------------------------------------
