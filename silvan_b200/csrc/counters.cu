@@ -324,9 +324,8 @@ __device__ void fold_node(const JobCounters &jc, const ApplyArgs &a, uint32_t no
 
 // Shared memory of phase D: the sub-round's per-sample factors (read by every
 // fold in place of global gathers), warp 0's large bucket in sample order, and
-// one fold scratch per warp.  The factors arrive by bulk copies, which start
-// on a 16-byte boundary: s_inv holds samples from lo & ~1 on, s_sgn from
-// lo & ~3 on (inv_base / sgn_base).
+// one fold scratch per warp.  s_inv holds samples from lo & ~1 on, s_sgn
+// from lo & ~3 on (inv_base / sgn_base).
 struct CommitSmem {
     double s_inv[kLargeBucket + 2];         // 1 / num_paths of the sub-round's samples
     uint32_t s_sgn[kLargeBucket + 4];       // their Rademacher signs (pass 2)
@@ -334,66 +333,22 @@ struct CommitSmem {
     uint32_t bits[kLargeBucket / 32];       // samples of that bucket
     uint32_t wpre[kLargeBucket / 32];       // set bits before each word
     FoldScratch fsc[kCommitThreads / 32];
-    unsigned long long mbar;                // completion of the bulk copies
 };
-static_assert(offsetof(CommitSmem, s_sgn) % 16 == 0, "bulk copy destination alignment");
 constexpr size_t kCommitSmem = sizeof(CommitSmem);
 __device__ __forceinline__ uint32_t inv_base(const ApplyArgs &a) { return a.lo & ~1u; }
 __device__ __forceinline__ uint32_t sgn_base(const ApplyArgs &a) { return a.lo & ~3u; }
-constexpr uint32_t kStagePolls = 1u << 22;  // polls of the bulk-copy wait (microseconds in practice)
 
-// The sub-round's 1 / num_paths and signs into shared memory: two bulk
-// copies (cp.async.bulk, no multicast) that thread 0 issues, completing on an
-// mbarrier that every thread waits for with a bounded poll.  Both sources are
-// whole 16-byte units inside the per-sample arrays (max_samples is a
-// multiple of 4); where that cannot hold, the threads copy with plain loads.
-// False when the wait ran out.
-__device__ bool stage_factors(const RoundBuffers &rb, const ApplyArgs &a, CommitSmem &sm) {
-    const uint32_t i0 = inv_base(a), i1 = (a.hi + 1u) & ~1u;
-    const uint32_t s0 = sgn_base(a), s1 = (a.hi + 3u) & ~3u;
-    const bool pass2 = a.pass == 2;
-    const bool bulk = i1 <= rb.max_samples && s1 <= rb.max_samples &&
-                      ((uintptr_t)(rb.inv_np + i0) & 15u) == 0 &&
-                      ((uintptr_t)(rb.signs + s0) & 15u) == 0;
-    if (!bulk) {
-        for (uint32_t i = threadIdx.x; i < i1 - i0; i += blockDim.x)
-            sm.s_inv[i] = i0 + i < rb.max_samples ? __ldcg(&rb.inv_np[i0 + i]) : 0.0;
-        for (uint32_t i = threadIdx.x; i < s1 - s0; i += blockDim.x)
-            sm.s_sgn[i] = pass2 && s0 + i < rb.max_samples ? __ldcg(&rb.signs[s0 + i]) : 0u;
-        __syncthreads();
-        return true;
-    }
-    const uint32_t mb = (uint32_t)__cvta_generic_to_shared(&sm.mbar);
-    if (threadIdx.x == 0) {
-        const uint32_t inv_bytes = 8u * (i1 - i0), sgn_bytes = pass2 ? 4u * (s1 - s0) : 0u;
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mb) : "memory");
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mb),
-                     "r"(inv_bytes + sgn_bytes)
-                     : "memory");
-        asm volatile(
-            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, "
-            "[%3];" ::"r"((uint32_t)__cvta_generic_to_shared(sm.s_inv)),
-            "l"(rb.inv_np + i0), "r"(inv_bytes), "r"(mb)
-            : "memory");
-        if (pass2)
-            asm volatile(
-                "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], "
-                "%2, [%3];" ::"r"((uint32_t)__cvta_generic_to_shared(sm.s_sgn)),
-                "l"(rb.signs + s0), "r"(sgn_bytes), "r"(mb)
-                : "memory");
-    }
-    __syncthreads();  // the barrier is initialised before anyone polls it
-    uint32_t done = 0;
-    for (uint32_t i = 0; i < kStagePolls && !done; i++)
-        asm volatile(
-            "{\n\t.reg .pred p;\n\t"
-            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n\t"
-            "selp.u32 %0, 1, 0, p;\n\t}"
-            : "=r"(done)
-            : "r"(mb)
-            : "memory");
-    return __syncthreads_and(done) != 0;
+// The sub-round's 1 / num_paths and signs into shared memory, read with
+// L2-coherent loads: phase A wrote them from other CTAs, ordered before this
+// read by the grid barrier.
+__device__ void stage_factors(const RoundBuffers &rb, const ApplyArgs &a, CommitSmem &sm) {
+    const uint32_t i0 = inv_base(a), i1 = min((a.hi + 1u) & ~1u, rb.max_samples);
+    const uint32_t s0 = sgn_base(a), s1 = min((a.hi + 3u) & ~3u, rb.max_samples);
+    for (uint32_t i = threadIdx.x; i < i1 - i0; i += blockDim.x)
+        sm.s_inv[i] = __ldcg(&rb.inv_np[i0 + i]);
+    for (uint32_t i = threadIdx.x; i < s1 - s0; i += blockDim.x)
+        sm.s_sgn[i] = a.pass == 2 ? __ldcg(&rb.signs[s0 + i]) : 0u;
+    __syncthreads();
 }
 constexpr int kLoads = 8;  // bucket entries a lane of warp 0 loads at once
 constexpr uint32_t kSmallWarps = kCommitThreads / 32 - 1;  // warps 1.. of each CTA
@@ -623,7 +578,7 @@ __global__ void __launch_bounds__(kCommitThreads, 1) commit_round_kernel(const A
         CommitSmem &sm = *reinterpret_cast<CommitSmem *>(commit_smem);
         // the sub-round's factors into shared memory, then warp 0 folds the
         // large buckets while the other warps fold the small ones
-        if (!stage_factors(rb, a, sm)) goto timeout;
+        stage_factors(rb, a, sm);
         if (threadIdx.x < 32) apply_large(rb, jc, jr, a, sm);
         else apply_small(rb, jc, jr, a, T, sm);
         __syncthreads();

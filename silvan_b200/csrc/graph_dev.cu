@@ -5,10 +5,16 @@ namespace silvan {
 
 namespace {
 
-__global__ void narrow_offsets_kernel(const uint64_t *in, uint32_t *out, uint32_t count) {
+// Offsets above the entry count are clamped to it and flagged, so that no
+// later kernel reads past the adjacency array.
+__global__ void narrow_offsets_kernel(const uint64_t *in, uint32_t *out, uint32_t count,
+                                      uint64_t limit, uint32_t *bad) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count;
-         i += gridDim.x * blockDim.x)
-        out[i] = (uint32_t)in[i];
+         i += gridDim.x * blockDim.x) {
+        const uint64_t v = in[i];
+        if (v > limit) atomicOr(bad, 1u);
+        out[i] = (uint32_t)(v > limit ? limit : v);
+    }
 }
 
 // one warp per row
@@ -39,8 +45,9 @@ cudaError_t make_rows(const uint32_t *off, uint2 *rows, uint32_t n, cudaStream_t
     return cudaGetLastError();
 }
 
-cudaError_t narrow_offsets(const uint64_t *in, uint32_t *out, uint32_t count, cudaStream_t s) {
-    narrow_offsets_kernel<<<592, 256, 0, s>>>(in, out, count);
+cudaError_t narrow_offsets(const uint64_t *in, uint32_t *out, uint32_t count, uint64_t limit,
+                           uint32_t *bad, cudaStream_t s) {
+    narrow_offsets_kernel<<<592, 256, 0, s>>>(in, out, count, limit, bad);
     return cudaGetLastError();
 }
 

@@ -7,7 +7,8 @@
 
 namespace silvan {
 
-cudaError_t narrow_offsets(const uint64_t *in, uint32_t *out, uint32_t count, cudaStream_t s);
+cudaError_t narrow_offsets(const uint64_t *in, uint32_t *out, uint32_t count, uint64_t limit,
+                           uint32_t *bad, cudaStream_t s);
 // rows[v] = (off[v], off[v + 1]) for v < n: a row's bounds in one 8-byte load
 // (one memory transaction where two 4-byte loads take two).
 cudaError_t make_rows(const uint32_t *off, uint2 *rows, uint32_t n, cudaStream_t s);

@@ -421,8 +421,9 @@ __device__ void expand_level(const SegDesc &A, SamplerSmem<BLOCK> &s, NodeRec *r
             // on R-MAT); their whole record is then written by the joining
             // hit with one store in phase 2, and only nodes with several hits
             // get the sigma and last-key atomics.  The tiles of a level run
-            // one after another on this CTA, so a later tile's hits find the
-            // record complete and add to it.
+            // one after another on this CTA, separated by a barrier after
+            // each tile's stores, so a later tile's hits find the record
+            // complete and add to it.
 #pragma unroll
             for (int k = 0; k < kItems; k++) {
                 if (code[k] != 1) continue;
@@ -545,6 +546,11 @@ __device__ void expand_level(const SegDesc &A, SamplerSmem<BLOCK> &s, NodeRec *r
                     if (pos < kMeetCap) meet[pos] = make_uint2(xs[k], ys[k]);
                 }
             }
+            // A single-hit record is written whole by its joining hit; a hit
+            // of the next tile on the same node must find it written and add
+            // to it, not be overwritten by it (the chunk's last tile has the
+            // barrier below).
+            if (t0 + (uint32_t)kTile < G) __syncthreads();
         }
         if (threadIdx.x == 0) s.vis += G;
         gbase += G;
