@@ -83,7 +83,7 @@ typedef struct {
                             entries are expanded by several sampler CTAs
                             together (same results): 0 = default (128 x the
                             CTA size while samples remain to be handed out,
-                            16 x once all are taken), 0xffffffff = never    */
+                            64 x once all are taken), 0xffffffff = never    */
     uint32_t wait_polls; /* polls after which a wait between the CTAs that
                             share a level gives up (the sample then reports
                             SILVAN_E_TIMEOUT and the job fails; later jobs

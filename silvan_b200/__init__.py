@@ -379,7 +379,7 @@ class Probabilistic:
     ("reference", or "sigma" for path-count-weighted predecessors),
     `assist_items` (BFS levels of at least this many adjacency entries are
     expanded by several sampler CTAs; 0 = 128 x the CTA size while samples
-    remain, 16 x once all are taken, 0xFFFFFFFF =
+    remain, 64 x once all are taken, 0xFFFFFFFF =
     never) and `wait_polls` (polls after which a wait between CTAs that
     share a level gives up and the job fails with E_TIMEOUT; 0 = default,
     0xFFFFFFFF = no polls, a hook for tests of that path) and

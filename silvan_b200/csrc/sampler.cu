@@ -783,8 +783,9 @@ __device__ __forceinline__ int32_t post_level(const SamplerLaunch &L, SamplerSme
     const uint32_t items = depth == 0 ? r0.y - r0.x : (side_u ? s.sum_u : s.sum_v);
     const uint32_t F = hi - lo;
     // Default threshold: 32 tiles while the round still has samples to hand
-    // out, four tiles once every sample is taken (on R-MAT scale 20 two
-    // tiles took 3 % longer, eight tiles while samples remain 5 % longer).  While samples remain, every
+    // out, 16 tiles once every sample is taken (on R-MAT scale 20, over 60
+    // seeds: 16 and 24 tiles alike, 8 tiles 5 % longer, 4 tiles 7 %, 2 tiles
+    // 10 %; eight tiles while samples remain 5 % longer).  While samples remain, every
     // CTA is busy with its own and helps only between samples, and a shared
     // tile costs more than one expanded alone (the look-backs and the tile
     // table), so only levels long enough to become the launch's tail are
@@ -793,7 +794,7 @@ __device__ __forceinline__ int32_t post_level(const SamplerLaunch &L, SamplerSme
     uint32_t thr = A.assist_items;
     if (thr == kAssistItemsAuto) {
         const bool draining = ld_acquire_u32(&L.hdr->work) >= L.hdr->total;
-        thr = (draining ? 4u : 32u) * (uint32_t)Shape<BLOCK>::kTile;
+        thr = (draining ? 16u : 32u) * (uint32_t)Shape<BLOCK>::kTile;
     }
     if (items < thr || F > L.assist.node_cap ||
         (uint64_t)items / Shape<BLOCK>::kTile + F / Shape<BLOCK>::kChunk + 2u > L.assist.tile_cap)
