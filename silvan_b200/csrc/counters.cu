@@ -807,13 +807,6 @@ __device__ __forceinline__ int32_t peel_index_of(const JobCounters &jc, uint32_t
     return idx;
 }
 
-__global__ void peel_index_kernel(JobCounters jc, uint32_t n, double m, double a, uint32_t *unc,
-                                  uint32_t *n_unc, uint32_t cap) {
-    const double la = log(a);
-    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x)
-        peel_index_of(jc, v, m, la, unc, n_unc, cap);
-}
-
 // The end of pass 1 in one kernel: with peeling (nbins > 0) every node's
 // index, the uncertain list and the histogram of the indices over
 // [idx_min, idx_min + nbins) (hist and n_unc zeroed before); the last CTA
@@ -936,14 +929,6 @@ cudaError_t stop_reduce_init(StopReduction *acc, uint32_t *ticket, cudaStream_t 
 cudaError_t stop_reduce(const JobCounters &jc, int nparts, uint32_t D, StopReduction *acc,
                         uint32_t *ticket, const StopReadback &out, cudaStream_t stream) {
     stop_reduce_kernel<<<296, 512, 0, stream>>>(jc, nparts, D, acc, ticket, out);
-    return cudaGetLastError();
-}
-
-cudaError_t peel_index(const JobCounters &jc, uint32_t n, double num_samples, double a,
-                       uint32_t *uncertain, uint32_t *n_uncertain, uint32_t cap,
-                       cudaStream_t stream) {
-    cudaMemsetAsync(n_uncertain, 0, sizeof(uint32_t), stream);
-    peel_index_kernel<<<592, 256, 0, stream>>>(jc, n, num_samples, a, uncertain, n_uncertain, cap);
     return cudaGetLastError();
 }
 

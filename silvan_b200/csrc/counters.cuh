@@ -160,12 +160,6 @@ cudaError_t stop_reduce_init(StopReduction *acc, uint32_t *ticket, cudaStream_t 
 cudaError_t stop_reduce(const JobCounters &jc, int nparts, uint32_t D, StopReduction *acc,
                         uint32_t *ticket, const StopReadback &out, cudaStream_t stream);
 
-// Empirical peeling index of every node (Probabilistic.cpp:855-862), with the
-// nodes whose index is within rounding distance of a boundary listed so that
-// the host can recompute them with the C library's log.
-cudaError_t peel_index(const JobCounters &jc, uint32_t n, double num_samples, double a,
-                       uint32_t *uncertain, uint32_t *n_uncertain, uint32_t cap,
-                       cudaStream_t stream);
 cudaError_t peel_map(const JobCounters &jc, uint32_t n, const int32_t *lut, int32_t idx_min,
                      int32_t lut_size, uint32_t *hist, cudaStream_t stream);
 cudaError_t peel_hist(const JobCounters &jc, uint32_t n, int32_t idx_min, int32_t nbins,
@@ -179,10 +173,13 @@ struct Pass1Readback {
     uint32_t *hist;    // nbins peeling-index counts
     uint32_t *n_unc;   // uncertain indices listed
 };
-// One kernel: peel_index and peel_hist when nbins > 0 (hist and n_uncertain
-// are zeroed here), then the histogram, the uncertain count, the scalars and
-// the path-length counts copied to `out`.  ticket is a zero word that the
-// kernel leaves zero.
+// One kernel: when nbins > 0, every node's peeling index
+// (Probabilistic.cpp:855-862), the nodes whose index lies within rounding
+// distance of a boundary (listed so that the host recomputes them with the C
+// library's log) and the histogram of the indices (hist and n_uncertain are
+// zeroed here); then the histogram, the uncertain count, the scalars and the
+// path-length counts copied to `out`.  ticket is a zero word that the kernel
+// leaves zero.
 cudaError_t pass1_readback(const JobCounters &jc, uint32_t n, double num_samples, double a,
                            int32_t idx_min, int32_t nbins, uint32_t *hist, uint32_t *uncertain,
                            uint32_t *n_uncertain, uint32_t cap, uint32_t D, uint32_t *ticket,
